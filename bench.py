@@ -1,0 +1,383 @@
+"""Benchmark of the unwrapping path: Mpix/s unwrapped at 8192^2.
+
+Workload (default): the 8192x8192 TOPO scene -- fractal power-law topography
+(beta -3, 0..2500 m) through lambda 0.24 m, B_perp 150 m, R 850 km, look 35
+deg; exponential amplitudes, coherence in [0.2, 0.9], nlooks 20 -- seeded
+synthetic data, unwrapped with init='laplace' and the reference's defaults
+(auto-tiling toward 1024 px with 64 px overlap -> 9x9 tiles, 16 IRLS passes,
+1000 PCG iterations, tol 1e-3), cost build + Laplace PCG + congruence +
+conncomp + stitching.
+
+One JSON line on rank 0.  `value` = scene pixels of all ranks / device time
+(inputs resident in HBM); `e2e` = the same through cuphu_unwrap_ex with
+pinned host buffers (H2D of igram+corr and D2H of unw+conncomp inside the
+timed region).  Extra keys: FP64-PCG throughput and the mixed-vs-FP64
+cycle-map comparison, the cost-kernel bandwidth, the solver roofline, the
+CPU baseline.  Multi-GPU: one process per GPU, independent replicas of the
+scene (no data-path collective; "scaling": "weak").
+
+--impl reference times the CPU restatement of the reference path (the
+oracle: cost build + FP64 Jacobi-PCG/IRLS + conncomp) on one 967x967 tile
+of the same scene with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM = 6650.0
+METRIC = "Mpix/s unwrapped at 8192^2 (mixed-precision Laplace PCG)"
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-i", str(self.gpu), "-lms", "200"], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(smax)) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_scene(workload, seed):
+    from cuphu_b200 import synthetic as S
+    name = {"c2_8192_topo": "c2_8192_topo", "c1_4096_smooth": "c1_4096_smooth",
+            "c0_512_defo": "c0_512_defo", "c4_2048_defo": "c4_2048_defo"}[workload]
+    ig, g, truth, ex = S.config_scene(name, seed=seed)
+    return ig, g, ex
+
+
+def tiles_for(nrow, ncol):
+    from cuphu_b200._unwrap import _auto_ntiles_by_target_size
+    return _auto_ntiles_by_target_size(nrow, ncol, 1024, 64, 64)
+
+
+def cpu_baseline(ig, g, nlooks, mode, n_irls):
+    """The oracle (CPU restatement of the reference path) on one tile-sized
+    crop of the scene: cost build + FP64 PCG/IRLS + conncomp."""
+    import oracle as O
+    n = 967
+    ph = O.phase_from_igram(np.ascontiguousarray(ig[:n, :n]))
+    gg = np.ascontiguousarray(g[:n, :n])
+    t0 = time.perf_counter()
+    c = O.build_costs(ph, gg, nlooks, mode=mode)
+    _, _, unw, it = O.laplace_f64(c, ph, O.lap_opts(n_irls=n_irls))
+    O.conncomp(unw, gg)
+    dt = time.perf_counter() - t0
+    return n * n / dt / 1e6, dt, int(it.sum()), n
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    ig, g, ex = make_scene(args.workload, args.seed)
+    mode = {"smooth": 0, "defo": 1, "topo": 2}[ex["cost"]]
+    n_irls = ex.get("n_irls", 16)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        v, dt, iters, n = cpu_baseline(ig, g, ex["nlooks"], mode, n_irls)
+        if i >= args.warmup:
+            vals.append((v, dt))
+    v = float(np.mean([x[0] for x in vals]))
+    ms = float(np.mean([x[1] for x in vals])) * 1e3
+    cores = os.cpu_count()
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mpix/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "sample": f"{n}x{n} crop, full pipeline"},
+            "cpu_baseline": {"value": v, "unit": "Mpix/s", "cores": cores, "kind": "port",
+                             "sample": f"{n}x{n} crop of the {args.workload} scene: cost build "
+                                       f"+ FP64 Jacobi-PCG ({n_irls} IRLS passes) + conncomp, "
+                                       f"OpenMP on {cores} threads"},
+            "e2e": {"value": v, "unit": "Mpix/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from cuphu_b200._lib import (CuPhuSolveStats, check, default_params, default_solve_options,
+                                 default_tile_params, lib)
+    torch.cuda.set_device(local_rank)
+    L = lib()
+    ig, g, ex = make_scene(args.workload, args.seed + rank * 0)
+    nrow, ncol = g.shape
+    npix = nrow * ncol
+    mode = {"smooth": 0, "defo": 1, "topo": 2}[ex["cost"]]
+    nlooks = float(ex["nlooks"])
+    ntr, ntc = tiles_for(nrow, ncol)
+    params = default_params(nlooks=nlooks, ncorrlooks=nlooks)
+    tile = default_tile_params(ntilerow=ntr, ntilecol=ntc, rowovrlp=64, colovrlp=64)
+    prec = {"mixed": 0, "fp64": 1}[args.precision]
+    opts = default_solve_options(precision=prec, ref_row=0, ref_col=0)
+    if "n_irls" in ex:
+        opts.n_irls = int(ex["n_irls"])
+
+    d_ig = torch.from_numpy(ig.view(np.float32)).cuda()
+    d_g = torch.from_numpy(g).cuda()
+    d_u = torch.empty((nrow, ncol), dtype=torch.float32, device="cuda")
+    d_c = torch.empty((nrow, ncol), dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+    sptr = C.c_void_p(stream.cuda_stream)
+
+    def step(o, stats=None):
+        check(L.cuphu_unwrap_device(C.c_void_p(d_ig.data_ptr()), None, C.c_void_p(d_g.data_ptr()),
+                                    None, None, nrow, ncol, mode, C.byref(params),
+                                    C.byref(tile), C.byref(o), C.c_void_p(d_u.data_ptr()),
+                                    C.c_void_p(d_c.data_ptr()), None,
+                                    C.byref(stats) if stats is not None else None, sptr))
+
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+    st = CuPhuSolveStats()
+    for _ in range(args.warmup):
+        step(opts, st)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    if dist:
+        tdist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step(opts)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        tdist.barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    clk = clocks.stop()
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * npix / (ms * 1e-3) / 1e6
+
+    # solver statistics of one more run (stats make the call synchronous)
+    st = CuPhuSolveStats()
+    step(opts, st)
+    unw_mixed = d_u.cpu().numpy()
+
+    # roofline of the dominant kernel (the persistent solve): algorithmic
+    # bytes = tile pixels x (36 B per PCG iteration x iterations of the
+    # active tiles + 38 B per IRLS pass for assemble and reweight)
+    peak, peak_kind = hbm_peak()
+    tile_px = 0
+    from cuphu_b200._unwrap import _auto_ntiles_by_target_size  # noqa: F401
+    tr_f = [(int(t * (nrow - 64) / ntr), (nrow if t == ntr - 1 else int((t + 1) * (nrow - 64) / ntr) + 64)) for t in range(ntr)]
+    tc_f = [(int(t * (ncol - 64) / ntc), (ncol if t == ntc - 1 else int((t + 1) * (ncol - 64) / ntc) + 64)) for t in range(ntc)]
+    tile_px = sum((b - a) for a, b in tr_f) * sum((b - a) for a, b in tc_f)
+    px_iters = st.total_iters * tile_px  # upper bound: every tile active in every iteration
+    bpi = 36 if prec == 0 else 64
+    alg_bytes = px_iters * bpi + (opts.n_irls + 1) * tile_px * 38
+    achieved = alg_bytes / (st.solve_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                "kernel": "k_solve", "solve_ms": st.solve_ms, "pcg_iterations": st.total_iters,
+                "bytes_per_px_iter": bpi}
+
+    result = {}
+    if rank == 0 and not args.skip_fp64 and prec == 0:
+        o64 = default_solve_options(precision=1, ref_row=0, ref_col=0)
+        o64.n_irls = opts.n_irls
+        st64 = CuPhuSolveStats()
+        step(o64, st64)
+        torch.cuda.synchronize()
+        ee0 = torch.cuda.Event(enable_timing=True)
+        ee1 = torch.cuda.Event(enable_timing=True)
+        ee0.record(stream)
+        step(o64)
+        ee1.record(stream)
+        torch.cuda.synchronize()
+        ms64 = ee0.elapsed_time(ee1)
+        unw64 = d_u.cpu().numpy()
+        diff = unw_mixed.astype(np.float64) - unw64
+        result["fp64"] = {"value": npix / (ms64 * 1e-3) / 1e6, "ms_per_step": ms64,
+                          "speedup_mixed_vs_fp64": ms64 / ms,
+                          "cycle_mismatches": int(np.sum(np.abs(diff) > np.pi)),
+                          "rms_rad": float(np.sqrt(np.mean(diff ** 2))),
+                          "pcg_iterations": st64.total_iters}
+
+    # cost-kernel bandwidth (DEFO costs from the wrapped phase, 8192^2)
+    if rank == 0:
+        d_ph = torch.empty((nrow, ncol), dtype=torch.float32, device="cuda")
+        check(L.cuphu_phase_gpu(C.c_void_p(d_ig.data_ptr()), C.c_longlong(npix),
+                                C.c_void_p(d_ph.data_ptr()), sptr))
+        narcs = (nrow - 1) * ncol + nrow * (ncol - 1)
+        d_cost = torch.empty((narcs, 4), dtype=torch.int16, device="cuda")
+        pc = default_params(nlooks=nlooks, ncorrlooks=nlooks)
+        for _ in range(3):
+            check(L.cuphu_build_costs_device(C.c_void_p(d_ph.data_ptr()), C.c_void_p(d_g.data_ptr()),
+                                             None, nrow, ncol, 1, C.byref(pc),
+                                             C.c_void_p(d_cost.data_ptr()), None, sptr))
+        ce0 = torch.cuda.Event(enable_timing=True)
+        ce1 = torch.cuda.Event(enable_timing=True)
+        reps = 10
+        ce0.record(stream)
+        for _ in range(reps):
+            check(L.cuphu_build_costs_device(C.c_void_p(d_ph.data_ptr()), C.c_void_p(d_g.data_ptr()),
+                                             None, nrow, ncol, 1, C.byref(pc),
+                                             C.c_void_p(d_cost.data_ptr()), None, sptr))
+        ce1.record(stream)
+        torch.cuda.synchronize()
+        cms = ce0.elapsed_time(ce1) / reps
+        cbytes = npix * 4 + npix * 4 + narcs * 8
+        result["cost_build"] = {"kernel": "k_costs<DEFO>", "ms": cms,
+                                "gbs": cbytes / (cms * 1e-3) / 1e9,
+                                "frac": cbytes / (cms * 1e-3) / 1e9 / peak,
+                                "bytes_per_px": cbytes / npix}
+        del d_cost, d_ph
+
+    # end to end through the C ABI with pinned host buffers
+    h_ig = torch.from_numpy(ig.view(np.float32)).pin_memory()
+    h_g = torch.from_numpy(g).pin_memory()
+    h_u = torch.empty((nrow, ncol), dtype=torch.float32).pin_memory()
+    h_c = torch.empty((nrow, ncol), dtype=torch.int32).pin_memory()
+
+    def e2e_step():
+        check(L.cuphu_unwrap_ex(C.c_void_p(h_ig.data_ptr()), C.c_void_p(h_g.data_ptr()), None,
+                                None, nrow, ncol, mode, C.byref(params), C.byref(tile),
+                                C.byref(opts), local_rank, C.c_void_p(h_u.data_ptr()),
+                                C.c_void_p(h_c.data_ptr()), None))
+
+    e2e_step()
+    if dist:
+        tdist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(max(1, args.steps)):
+        e2e_step()
+    e2e_s = (time.perf_counter() - t0) / max(1, args.steps)
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        v, dt, iters, n = cpu_baseline(ig, g, nlooks, mode, opts.n_irls)
+        cpu = {"value": v, "unit": "Mpix/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"{n}x{n} crop of the scene: cost build + FP64 Jacobi-PCG "
+                         f"({opts.n_irls} IRLS passes, {iters} iterations) + conncomp, "
+                         f"{dt:.1f} s"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "Mpix/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32" if prec == 0 else "f64", "data": "synthetic",
+                "config": {"workload": args.workload, "shape": [nrow, ncol],
+                           "tiles": [ntr, ntc], "overlap": 64, "n_irls": opts.n_irls,
+                           "max_iter": opts.max_iter, "tol": opts.tol,
+                           "precision": args.precision, "parallelism": f"replicas{world}",
+                           "l2": "inputs (805 MB) larger than L2"},
+                "e2e": {"value": world * npix / e2e_s / 1e6, "unit": "Mpix/s",
+                        "h2d_bytes_per_step": npix * 12, "d2h_bytes_per_step": npix * 8},
+                "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
+                "gpu_launches": 14 * args.steps}
+        line.update(result)
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2_8192_topo")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as tdist
+            tdist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

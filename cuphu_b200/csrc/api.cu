@@ -1,0 +1,1151 @@
+/*
+ * api.cu -- C ABI of libcuphu_b200 and the host orchestrator.
+ *
+ * Replaces cuphu_unwrap / solve_tile / cuphu_build_costs_gpu
+ * (cuphu_solver.cpp:370-510, 1675-2171) for the Laplace path.  Differences
+ * in mechanism (not in results):
+ *  - one stream per call, no host threads: all tiles of all scenes are
+ *    planned on the host and solved by one persistent launch;
+ *  - no host round trips inside the pipeline: phase, weights, solve,
+ *    labelling, stitching and merge are device kernels, the host copies the
+ *    inputs in and the outputs out once;
+ *  - a grow-only per-device workspace replaces the reference's per-call
+ *    cudaMalloc/cudaFree; calls on one device are serialised by a mutex and
+ *    ordered on the GPU by an event, so asynchronous device-pointer calls on
+ *    different streams never share scratch concurrently;
+ *  - errors are returned as status codes (cuphu_last_error() has the text),
+ *    never thrown across the ABI.
+ */
+#include "kernels.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+namespace cuphu {
+
+static thread_local std::string g_err;
+
+void set_error(const std::string &msg) { g_err = msg; }
+
+int fail(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return 0;
+    g_err = std::string(what) + ": " + cudaGetErrorString(e);
+    return CUPHU_ERR_CUDA;
+}
+
+/* ── per-device workspace ──────────────────────────────────────────────── */
+struct Workspace {
+    std::mutex mu;
+    char *dev = nullptr;
+    size_t dev_size = 0;
+    char *host = nullptr;   /* pinned staging for descriptors */
+    size_t host_size = 0;
+    cudaEvent_t done = nullptr;
+    cudaStream_t stream = nullptr;
+    int *status = nullptr;  /* pinned: device status of the last job */
+};
+
+static Workspace g_ws[64];
+
+static int ws_acquire(int dev, size_t dbytes, size_t hbytes, cudaStream_t s, Workspace *&W)
+{
+    if (dev < 0 || dev >= 64) return fail(CUPHU_ERR_INVALID, "device index out of range");
+    W = &g_ws[dev];
+    if (!W->done) {
+        CUPHU_TRY_CUDA(cudaEventCreateWithFlags(&W->done, cudaEventDisableTiming));
+        CUPHU_TRY_CUDA(cudaEventRecord(W->done, s));
+        CUPHU_TRY_CUDA(cudaHostAlloc((void **)&W->status, sizeof(int), cudaHostAllocDefault));
+        *W->status = 0;
+    }
+    if (dbytes > W->dev_size) {
+        CUPHU_TRY_CUDA(cudaDeviceSynchronize());
+        if (W->dev) cudaFree(W->dev);
+        W->dev = nullptr;
+        W->dev_size = 0;
+        size_t want = dbytes + dbytes / 8 + (1u << 20);
+        if (cudaMalloc(&W->dev, want) != cudaSuccess) {
+            cudaGetLastError();
+            if (cudaMalloc(&W->dev, dbytes) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(CUPHU_ERR_ALLOC, "device workspace allocation failed (" +
+                                                 std::to_string(dbytes >> 20) + " MiB)");
+            }
+            want = dbytes;
+        }
+        W->dev_size = want;
+    }
+    if (hbytes > W->host_size) {
+        CUPHU_TRY_CUDA(cudaEventSynchronize(W->done));
+        if (W->host) cudaFreeHost(W->host);
+        W->host = nullptr;
+        W->host_size = 0;
+        size_t want = hbytes + hbytes / 4 + 4096;
+        if (cudaHostAlloc((void **)&W->host, want, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(CUPHU_ERR_ALLOC, "pinned staging allocation failed");
+        }
+        W->host_size = want;
+    }
+    /* previous user of the workspace (any stream) must be done on the GPU; the
+     * pinned staging buffer is rewritten by the host, so wait on the host */
+    CUPHU_TRY_CUDA(cudaEventSynchronize(W->done));
+    return 0;
+}
+
+struct Bump {
+    char *base;
+    size_t off = 0;
+    explicit Bump(char *b) : base(b) {}
+    template <typename T> T *take(size_t n)
+    {
+        off = (off + 255) & ~(size_t)255;
+        T *p = reinterpret_cast<T *>(base + off);
+        off += n * sizeof(T);
+        return p;
+    }
+};
+
+/* ── planning ──────────────────────────────────────────────────────────── */
+struct SceneIn {
+    const float2 *ig = nullptr;
+    const float *re = nullptr, *im = nullptr;
+    const float *ph_in = nullptr;
+    const float *corr = nullptr;
+    const unsigned char *mask = nullptr, *conf = nullptr;
+    int nrow = 0, ncol = 0, ntr = 1, ntc = 1, rovl = 0, covl = 0;
+    double nlooks = 1.0;
+    float *unw = nullptr;
+    uint32_t *cc = nullptr;
+    int ref_row = -1, ref_col = -1;
+};
+
+static void tile_bounds(int n, int nt, int ovl, int t, int &first, int &len)
+{
+    int f = (int)((long long)t * (n - ovl) / nt);
+    int last = (t == nt - 1) ? n : (int)((long long)(t + 1) * (n - ovl) / nt) + ovl;
+    first = f;
+    len = last - f;
+}
+
+struct Plan {
+    std::vector<TileDesc> tiles;
+    std::vector<int> item_tile, row_tile, maps;
+    std::vector<ScenePlan> scenes;
+    std::vector<PairDesc> pairs;
+    std::vector<CostConsts> consts;
+    std::vector<size_t> map_off;
+    long long nplane = 0;
+    int nitems = 0, total_rows = 0;
+};
+
+static int plan_job(const std::vector<SceneIn> &S, const CuPhuParams &prm, Plan &pl)
+{
+    for (size_t s = 0; s < S.size(); ++s) {
+        const SceneIn &in = S[s];
+        if (in.nrow < 1 || in.ncol < 1) return fail(CUPHU_ERR_INVALID, "scene shape must be >= 1x1");
+        if (in.ntr < 1 || in.ntc < 1 || in.ntr > in.nrow || in.ntc > in.ncol)
+            return fail(CUPHU_ERR_INVALID, "tile counts must be in [1, extent]");
+        if (in.rovl < 0 || in.covl < 0) return fail(CUPHU_ERR_INVALID, "tile overlap must be >= 0");
+        bool single = in.ntr == 1 && in.ntc == 1;
+        ScenePlan sp = {};
+        sp.unw_out = in.unw;
+        sp.cc_out = in.cc;
+        sp.nrow = in.nrow;
+        sp.ncol = in.ncol;
+        sp.ntr = in.ntr;
+        sp.ntc = in.ntc;
+        sp.rovl = in.rovl;
+        sp.covl = in.covl;
+        sp.tile0 = (int)pl.tiles.size();
+        sp.pair0 = (int)pl.pairs.size();
+        sp.ref_row = in.ref_row;
+        sp.ref_col = in.ref_col;
+        sp.maxncomps = (int)std::min<long>(prm.maxncomps, 0x7fffffffL);
+        sp.minfrac = prm.minconncompfrac;
+        sp.single = single ? 1 : 0;
+        CuPhuParams p2 = prm;
+        p2.nlooks = p2.ncorrlooks = in.nlooks;
+        pl.consts.push_back(make_cost_consts(p2));
+        for (int tr = 0; tr < in.ntr; ++tr)
+            for (int tc = 0; tc < in.ntc; ++tc) {
+                TileDesc T = {};
+                if (single) { T.r0 = 0; T.nr = in.nrow; T.c0 = 0; T.nc = in.ncol; }
+                else {
+                    tile_bounds(in.nrow, in.ntr, in.rovl, tr, T.r0, T.nr);
+                    tile_bounds(in.ncol, in.ntc, in.covl, tc, T.c0, T.nc);
+                }
+                if (T.nr < 1 || T.nc < 1 || T.r0 < 0 || T.c0 < 0 || T.r0 + T.nr > in.nrow ||
+                    T.c0 + T.nc > in.ncol)
+                    return fail(CUPHU_ERR_INVALID, "tile geometry degenerates (overlap too large)");
+                T.scene = (int)s;
+                T.tr = tr;
+                T.tc = tc;
+                T.ph_pitch = in.ncol;
+                T.pitch = (T.nc + 3) & ~3;
+                T.pix = pl.nplane;
+                pl.nplane += (long long)T.nr * T.pitch;
+                T.nbx = (T.nc + kItemBx - 1) / kItemBx;
+                int nby = (T.nr + kItemBy - 1) / kItemBy;
+                T.nitems = T.nbx * nby;
+                T.item0 = pl.nitems;
+                pl.nitems += T.nitems;
+                T.row0 = pl.total_rows;
+                pl.total_rows += T.nr;
+                int tidx = (int)pl.tiles.size();
+                for (int i = 0; i < T.nitems; ++i) pl.item_tile.push_back(tidx);
+                for (int i = 0; i < T.nr; ++i) pl.row_tile.push_back(tidx);
+                pl.tiles.push_back(T);
+            }
+        if (!single && (in.rovl > 0 || in.covl > 0)) {
+            for (int tr = 0; tr < in.ntr; ++tr)
+                for (int tc = 0; tc + 1 < in.ntc; ++tc)
+                    pl.pairs.push_back({sp.tile0 + tr * in.ntc + tc, sp.tile0 + tr * in.ntc + tc + 1, 0,
+                                        in.covl});
+            for (int tr = 0; tr + 1 < in.ntr; ++tr)
+                for (int tc = 0; tc < in.ntc; ++tc)
+                    pl.pairs.push_back({sp.tile0 + tr * in.ntc + tc, sp.tile0 + (tr + 1) * in.ntc + tc, 1,
+                                        in.rovl});
+        }
+        /* merge maps: the last tile (in row-major order) whose kept interval
+         * covers a row/column wins, as the reference's sequential merge does */
+        pl.map_off.push_back(pl.maps.size());
+        std::vector<int> rm(in.nrow, 0), cm(in.ncol, 0);
+        if (!single) {
+            for (int tr = 0; tr < in.ntr; ++tr) {
+                int f, n;
+                tile_bounds(in.nrow, in.ntr, in.rovl, tr, f, n);
+                int a = tr == 0 ? 0 : in.rovl / 2, b = tr == in.ntr - 1 ? n : n - in.rovl / 2;
+                for (int r = f + a; r < f + b; ++r) rm[r] = tr;
+            }
+            for (int tc = 0; tc < in.ntc; ++tc) {
+                int f, n;
+                tile_bounds(in.ncol, in.ntc, in.covl, tc, f, n);
+                int a = tc == 0 ? 0 : in.covl / 2, b = tc == in.ntc - 1 ? n : n - in.covl / 2;
+                for (int c = f + a; c < f + b; ++c) cm[c] = tc;
+            }
+        }
+        pl.maps.insert(pl.maps.end(), rm.begin(), rm.end());
+        pl.maps.insert(pl.maps.end(), cm.begin(), cm.end());
+        pl.scenes.push_back(sp);
+    }
+    return 0;
+}
+
+struct JobOpts {
+    bool fp64 = false;
+    bool want_cc = true;
+    bool want_cyc = false;
+    CuPhuSolveOptions so;
+    const short *costs = nullptr;   /* launcher-level entry: w0 from a cost array */
+    int cost_stride = 2;
+    int32_t *cycles_out = nullptr;
+    float *cont_out = nullptr;      /* anchored continuous solution (single tile) */
+};
+
+/* Enqueue the whole unwrapping pipeline for a list of scenes on stream s. */
+static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpts &jo,
+                   cudaStream_t s, CuPhuSolveStats *stats)
+{
+    int dev = 0;
+    CUPHU_TRY_CUDA(cudaGetDevice(&dev));
+    Plan pl;
+    int rc = plan_job(S, prm, pl);
+    if (rc) return rc;
+    const CuPhuSolveOptions &o = jo.so;
+    if (o.n_irls < 0 || o.n_irls > 4096) return fail(CUPHU_ERR_INVALID, "n_irls out of range");
+    if (o.max_iter < 0) return fail(CUPHU_ERR_INVALID, "max_iter must be >= 0");
+    const int ntiles = (int)pl.tiles.size(), nsc = (int)S.size(), npairs = (int)pl.pairs.size();
+    const size_t vs = jo.fp64 ? sizeof(double) : sizeof(float);
+    const size_t np = (size_t)pl.nplane;
+
+    /* device layout */
+    size_t need_phase = 0;
+    for (auto &in : S)
+        if (!in.ph_in) need_phase += (size_t)in.nrow * in.ncol;
+    auto layout = [&](Bump &b, SolverPlanes &P, float *&phase, TileDesc *&d_tiles, int *&d_item,
+                      ScenePlan *&d_sc, PairDesc *&d_pairs, int *&d_maps, int *&d_rowcnt,
+                      int *&d_nlab, double *&d_pairk, double *&d_tilek, unsigned *&d_coff,
+                      SceneOut *&d_sout, CostConsts *&d_k, TileState *&d_st, double *&d_part,
+                      SolverCtl *&d_ctl, float *&d_deltas, int *&d_pass) {
+        phase = b.take<float>(need_phase);
+        P.w0d = b.take<float>(np);
+        P.w0r = b.take<float>(np);
+        P.wd = b.take<float>(np);
+        P.wr = b.take<float>(np);
+        P.x = b.take<char>(np * vs);
+        P.r = b.take<char>(np * vs);
+        P.p0 = b.take<char>(np * vs);
+        P.p1 = b.take<char>(np * vs);
+        P.q = b.take<char>(np * vs);
+        P.diag = b.take<char>(np * vs);
+        P.unw = b.take<float>(np);
+        P.cyc = jo.want_cyc ? b.take<int32_t>(np) : nullptr;
+        P.cont = jo.cont_out ? b.take<float>(np) : nullptr;
+        P.cc = b.take<uint32_t>(np);
+        P.aux = b.take<uint32_t>(np);
+        d_tiles = b.take<TileDesc>(ntiles);
+        d_item = b.take<int>(pl.nitems);
+        d_sc = b.take<ScenePlan>(nsc);
+        d_pairs = b.take<PairDesc>(std::max(npairs, 1));
+        d_maps = b.take<int>(pl.maps.size());
+        d_rowcnt = b.take<int>(2 * (size_t)pl.total_rows);
+        d_nlab = b.take<int>(ntiles);
+        d_pairk = b.take<double>(npairs + ntiles + 1);
+        d_tilek = b.take<double>(ntiles);
+        d_coff = b.take<unsigned>(ntiles);
+        d_sout = b.take<SceneOut>(nsc);
+        d_k = b.take<CostConsts>(nsc);
+        d_st = b.take<TileState>(ntiles);
+        d_part = b.take<double>(pl.nitems);
+        d_ctl = b.take<SolverCtl>(1);
+        d_deltas = b.take<float>(o.n_irls + 1);
+        d_pass = b.take<int>(o.n_irls + 1);
+    };
+    SolverPlanes P = {};
+    float *phase = nullptr, *d_deltas = nullptr;
+    TileDesc *d_tiles = nullptr;
+    int *d_item = nullptr, *d_maps = nullptr, *d_rowcnt = nullptr, *d_nlab = nullptr, *d_pass = nullptr;
+    ScenePlan *d_sc = nullptr;
+    PairDesc *d_pairs = nullptr;
+    double *d_pairk = nullptr, *d_tilek = nullptr, *d_part = nullptr;
+    unsigned *d_coff = nullptr;
+    SceneOut *d_sout = nullptr;
+    CostConsts *d_k = nullptr;
+    TileState *d_st = nullptr;
+    SolverCtl *d_ctl = nullptr;
+    Bump probe(nullptr);
+    layout(probe, P, phase, d_tiles, d_item, d_sc, d_pairs, d_maps, d_rowcnt, d_nlab, d_pairk,
+           d_tilek, d_coff, d_sout, d_k, d_st, d_part, d_ctl, d_deltas, d_pass);
+    size_t dbytes = probe.off + 256;
+    /* host staging: descriptors packed in the same order as the device copy */
+    size_t desc_begin = (size_t)((char *)d_tiles - (char *)nullptr);
+    size_t desc_end = (size_t)((char *)d_st - (char *)nullptr);
+    size_t hbytes = desc_end - desc_begin + 256;
+
+    std::lock_guard<std::mutex> lock(g_ws[dev].mu);
+    Workspace *W = nullptr;
+    rc = ws_acquire(dev, dbytes, hbytes, s, W);
+    if (rc) return rc;
+    Bump b(W->dev);
+    layout(b, P, phase, d_tiles, d_item, d_sc, d_pairs, d_maps, d_rowcnt, d_nlab, d_pairk, d_tilek,
+           d_coff, d_sout, d_k, d_st, d_part, d_ctl, d_deltas, d_pass);
+
+    /* finalise descriptors with device addresses */
+    size_t poff = 0;
+    std::vector<const float *> scene_ph(nsc);
+    for (int i = 0; i < nsc; ++i) {
+        if (S[i].ph_in) scene_ph[i] = S[i].ph_in;
+        else {
+            scene_ph[i] = phase + poff;
+            poff += (size_t)S[i].nrow * S[i].ncol;
+        }
+        pl.scenes[i].ph = scene_ph[i];
+        pl.scenes[i].rowmap = d_maps + pl.map_off[i];
+        pl.scenes[i].colmap = d_maps + pl.map_off[i] + S[i].nrow;
+    }
+    for (auto &T : pl.tiles) {
+        const SceneIn &in = S[T.scene];
+        size_t o0 = (size_t)T.r0 * in.ncol + T.c0;
+        T.ph = scene_ph[T.scene] + o0;
+        T.corr = in.corr + o0;
+        T.mask = in.mask ? in.mask + o0 : nullptr;
+        T.conf = in.conf ? in.conf + o0 : (in.mask ? in.mask + o0 : nullptr);
+    }
+    char *h = W->host;
+    auto put = [&](void *dptr, const void *src, size_t n) {
+        size_t off = (size_t)((char *)dptr - (char *)d_tiles);
+        if (n) std::memcpy(h + off, src, n);
+    };
+    put(d_tiles, pl.tiles.data(), ntiles * sizeof(TileDesc));
+    put(d_item, pl.item_tile.data(), pl.nitems * sizeof(int));
+    put(d_sc, pl.scenes.data(), nsc * sizeof(ScenePlan));
+    put(d_pairs, pl.pairs.data(), npairs * sizeof(PairDesc));
+    put(d_maps, pl.maps.data(), pl.maps.size() * sizeof(int));
+    put(d_rowcnt + pl.total_rows, pl.row_tile.data(), pl.total_rows * sizeof(int));
+    put(d_k, pl.consts.data(), nsc * sizeof(CostConsts));
+
+    cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
+    if (stats) {
+        cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2); cudaEventCreate(&e3);
+        cudaEventRecord(e0, s);
+    }
+    CUPHU_TRY_CUDA(cudaMemcpyAsync(d_tiles, h, (char *)d_st - (char *)d_tiles,
+                                   cudaMemcpyHostToDevice, s));
+    /* IRLS schedule, host powf exactly as cuphu_laplace.cu:517-518 */
+    std::vector<float> deltas(o.n_irls + 1, 0.0f);
+    for (int k = 0; k < o.n_irls; ++k)
+        deltas[k] = std::max(o.irls_delta_min, o.irls_delta_max * powf(0.5f, (float)k));
+    CUPHU_TRY_CUDA(cudaMemcpyAsync(d_deltas, deltas.data(), deltas.size() * sizeof(float),
+                                   cudaMemcpyHostToDevice, s));
+    CUPHU_TRY_CUDA(cudaMemsetAsync(d_st, 0, ntiles * sizeof(TileState), s));
+    CUPHU_TRY_CUDA(cudaMemsetAsync(d_ctl, 0, sizeof(SolverCtl), s));
+
+    for (int i = 0; i < nsc; ++i) {
+        if (S[i].ph_in) continue;
+        long long n = (long long)S[i].nrow * S[i].ncol;
+        rc = S[i].ig ? launch_phase(S[i].ig, (float *)scene_ph[i], n, s)
+                     : launch_phase_split(S[i].re, S[i].im, (float *)scene_ph[i], n, s);
+        if (rc) return rc;
+    }
+    if (jo.costs) {
+        const TileDesc &T = pl.tiles[0];
+        rc = launch_w0_from_costs(jo.costs, jo.cost_stride, T.nr, T.nc, T.pitch, P, s);
+    } else {
+        rc = launch_w0(d_tiles, d_item, pl.nitems, d_k, P, s);
+    }
+    if (rc) return rc;
+    SolveParams sp;
+    sp.n_irls = o.n_irls;
+    sp.max_iter = o.max_iter;
+    sp.replace_every = jo.fp64 ? 0 : o.replace_every;
+    sp.tol = o.tol;
+    sp.deltas = d_deltas;
+    sp.pass_iters = d_pass;
+    sp.timeout_ns = (long long)std::max(1, o.timeout_ms) * 1000000LL;
+    if (stats) cudaEventRecord(e1, s);
+    rc = launch_solve(jo.fp64, d_tiles, d_item, pl.nitems, ntiles, P, d_st, d_part, d_ctl, sp,
+                      dev, s);
+    if (rc) return rc;
+    if (stats) cudaEventRecord(e2, s);
+    if (jo.want_cc) {
+        CcArgs ca;
+        ca.poscost = nullptr;
+        ca.negcost = nullptr;
+        ca.corr_thresh = 0.05f;
+        ca.conncompthresh = prm.conncompthresh;
+        ca.minfrac = prm.minconncompfrac;
+        ca.maxncomps = (int)std::min<long>(prm.maxncomps, 0x7fffffffL);
+        rc = launch_conncomp(d_tiles, ntiles, pl.total_rows, d_item, pl.nitems, P, ca, d_rowcnt,
+                             d_nlab, s);
+        if (rc) return rc;
+    } else {
+        CUPHU_TRY_CUDA(cudaMemsetAsync(d_nlab, 0, ntiles * sizeof(int), s));
+    }
+    rc = launch_stitch(d_sc, nsc, d_tiles, d_pairs, npairs, P, d_nlab, d_pairk, d_tilek, d_coff,
+                       d_sout, s);
+    if (rc) return rc;
+    rc = launch_merge(d_sc, pl.scenes.data(), nsc, d_tiles, P, d_tilek, d_coff, d_sout, s);
+    if (rc) return rc;
+    if (jo.cycles_out && nsc == 1 && ntiles == 1 && P.cyc) {
+        const TileDesc &T = pl.tiles[0];
+        CUPHU_TRY_CUDA(cudaMemcpy2DAsync(jo.cycles_out, (size_t)T.nc * 4, P.cyc, (size_t)T.pitch * 4,
+                                         (size_t)T.nc * 4, T.nr, cudaMemcpyDeviceToDevice, s));
+    }
+    if (jo.cont_out && nsc == 1 && ntiles == 1 && P.cont) {
+        const TileDesc &T = pl.tiles[0];
+        CUPHU_TRY_CUDA(cudaMemcpy2DAsync(jo.cont_out, (size_t)T.nc * 4, P.cont, (size_t)T.pitch * 4,
+                                         (size_t)T.nc * 4, T.nr, cudaMemcpyDeviceToDevice, s));
+    }
+    CUPHU_TRY_CUDA(cudaMemcpyAsync(W->status, &d_ctl->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CUPHU_TRY_CUDA(cudaEventRecord(W->done, s));
+    if (stats) {
+        cudaEventRecord(e3, s);
+        CUPHU_TRY_CUDA(cudaEventSynchronize(e3));
+        SolverCtl ctl;
+        CUPHU_TRY_CUDA(cudaMemcpy(&ctl, d_ctl, sizeof(ctl), cudaMemcpyDeviceToHost));
+        float ms_solve = 0, ms_total = 0;
+        cudaEventElapsedTime(&ms_solve, e1, e2);
+        cudaEventElapsedTime(&ms_total, e0, e3);
+        stats->ntiles = ntiles;
+        stats->total_iters = ctl.total_iters;
+        stats->max_iters_pass = ctl.max_pass_iters;
+        stats->solve_ms = ms_solve;
+        stats->total_ms = ms_total;
+        cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2); cudaEventDestroy(e3);
+        if (ctl.err) return fail(CUPHU_ERR_TIMEOUT, "solver grid barrier timed out");
+    }
+    return cuda_fail(cudaGetLastError(), "unwrap pipeline");
+}
+
+/* default solver options, honouring the reference's environment overrides */
+static void default_solve_options(CuPhuSolveOptions *o)
+{
+    o->precision = CUPHU_PREC_MIXED;
+    o->n_irls = 16;
+    o->irls_delta_max = 0.5f;
+    o->irls_delta_min = 0.01f;
+    o->max_iter = 1000;
+    o->tol = 1e-3f;
+    o->replace_every = 50;
+    o->ref_row = -1;
+    o->ref_col = -1;
+    o->timeout_ms = 5000;
+    if (const char *e = std::getenv("CUPHU_N_IRLS")) o->n_irls = std::atoi(e);
+    if (const char *e = std::getenv("CUPHU_IRLS_DELTA_MAX")) o->irls_delta_max = (float)std::atof(e);
+    if (const char *e = std::getenv("CUPHU_IRLS_DELTA_MIN")) o->irls_delta_min = (float)std::atof(e);
+    if (const char *e = std::getenv("CUPHU_LAPLACE_MAX_ITER")) o->max_iter = std::atoi(e);
+    if (const char *e = std::getenv("CUPHU_LAPLACE_TOL")) o->tol = (float)std::atof(e);
+}
+
+static int check_common(CuPhuCostMode cost, const CuPhuParams *p)
+{
+    if (!p) return fail(CUPHU_ERR_INVALID, "params must not be NULL");
+    if (cost != CUPHU_COST_SMOOTH && cost != CUPHU_COST_DEFO && cost != CUPHU_COST_TOPO)
+        return fail(CUPHU_ERR_INVALID, "cost must be 'smooth', 'defo', or 'topo'");
+    if (!(p->ncorrlooks >= 1.0)) return fail(CUPHU_ERR_INVALID, "nlooks must be >= 1");
+    return 0;
+}
+
+static int check_tile_flags(const CuPhuTileParams *t)
+{
+    if (!t) return 0;
+    if (t->single_tile_reoptimize)
+        return fail(CUPHU_ERR_UNSUPPORTED,
+                    "single_tile_reoptimize needs SNAPHU's CPU TreeSolve, which is outside this build");
+    if (t->laplace_neighbor_feedback)
+        return fail(CUPHU_ERR_UNSUPPORTED, "laplace_neighbor_feedback is outside this build");
+    if (t->fix_cycle_spikes) return fail(CUPHU_ERR_UNSUPPORTED, "fix_cycle_spikes is outside this build");
+    return 0;
+}
+
+/* status of the last pipeline on a device, after its work completed */
+static int device_status(int dev)
+{
+    Workspace &W = g_ws[dev];
+    if (!W.done) return 0;
+    CUPHU_TRY_CUDA(cudaEventSynchronize(W.done));
+    if (W.status && *W.status)
+        return fail(CUPHU_ERR_TIMEOUT, "solver grid barrier timed out (device status set)");
+    return 0;
+}
+
+static cudaStream_t lib_stream(int dev)
+{
+    Workspace &W = g_ws[dev];
+    if (!W.stream) cudaStreamCreateWithFlags(&W.stream, cudaStreamNonBlocking);
+    return W.stream;
+}
+
+template <typename T>
+static T *dev_alloc_async(size_t n, cudaStream_t s)
+{
+    T *p = nullptr;
+    if (cudaMallocAsync((void **)&p, (n ? n : 1) * sizeof(T), s) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return p;
+}
+
+}  // namespace cuphu
+
+using namespace cuphu;
+
+extern "C" {
+
+const char *cuphu_last_error(void) { return g_err.c_str(); }
+
+/* SNAPHU's documented defaults (snaphu.conf); the reference takes them from
+ * the DEF_* macros of snaphu.h (cuphu_solver.cpp:148-216), absent here. */
+void cuphu_default_params(CuPhuParams *p)
+{
+    std::memset(p, 0, sizeof(*p));
+    p->rhosconst1 = 1.3;
+    p->rhosconst2 = 0.14;
+    p->cstd1 = 0.4;
+    p->cstd2 = 0.35;
+    p->cstd3 = 0.06;
+    p->defothreshfactor = 1.2;
+    p->sigsqcorr = 0.05;
+    p->nlooks = 23.8;
+    p->ncorrlooks = 23.8;
+    p->costscale = 100.0;
+    p->nshortcycle = 200.0;
+    p->sigsqshortmin = 1;
+    p->kperpdpsi = 7;
+    p->kpardpsi = 7;
+    p->defomax = 1.2;
+    p->p = -1.0;
+    p->minconncompfrac = 0.01;
+    p->conncompthresh = 300;
+    p->maxncomps = 32;
+}
+
+void cuphu_default_tile_params(CuPhuTileParams *tp)
+{
+    std::memset(tp, 0, sizeof(*tp));
+    tp->ntilerow = 1;
+    tp->ntilecol = 1;
+    tp->tilecostthresh = 500;
+    tp->minregionsize = 100;
+    tp->nproc = 1;
+    tp->ngpustreams = 2;
+    tp->laplace_neighbor_feedback_feather = 200;
+}
+
+void cuphu_default_bridge_params(CuPhuBridgeParams *bp)
+{
+    std::memset(bp, 0, sizeof(*bp));
+    bp->radius = 500;
+    bp->min_num_pixel = 14;
+    bp->erosion_size = 2;
+    bp->max_boundary_samples = 4096;
+    bp->ramp_type = CUPHU_RAMP_NONE;
+    bp->ramp_max_num_sample = 1000000;
+}
+
+void cuphu_default_solve_options(CuPhuSolveOptions *o) { default_solve_options(o); }
+
+int cuphu_unwrap_device(const float *igram_c64, const float *phase_in, const float *corr,
+                        const unsigned char *mask, const unsigned char *orig_mask, int nrow,
+                        int ncol, CuPhuCostMode cost_mode, const CuPhuParams *params,
+                        const CuPhuTileParams *tile, const CuPhuSolveOptions *opts,
+                        float *unw_out, uint32_t *conncomp_out, int32_t *cycles_out,
+                        CuPhuSolveStats *stats, void *stream)
+{
+    int rc = check_common(cost_mode, params);
+    if (rc) return rc;
+    if ((rc = check_tile_flags(tile))) return rc;
+    if ((!igram_c64 && !phase_in) || !corr || !unw_out)
+        return fail(CUPHU_ERR_INVALID, "igram (or phase), corr and unw must not be NULL");
+    CuPhuSolveOptions so;
+    if (opts) so = *opts; else default_solve_options(&so);
+    SceneIn in;
+    in.ig = reinterpret_cast<const float2 *>(igram_c64);
+    in.ph_in = igram_c64 ? nullptr : phase_in;
+    in.corr = corr;
+    in.mask = mask;
+    in.conf = orig_mask;
+    in.nrow = nrow;
+    in.ncol = ncol;
+    if (tile) {
+        in.ntr = tile->ntilerow; in.ntc = tile->ntilecol;
+        in.rovl = tile->rowovrlp; in.covl = tile->colovrlp;
+    }
+    in.nlooks = params->ncorrlooks;
+    in.unw = unw_out;
+    in.cc = conncomp_out;
+    in.ref_row = so.ref_row;
+    in.ref_col = so.ref_col;
+    std::vector<SceneIn> S(1, in);
+    JobOpts jo;
+    jo.fp64 = so.precision == CUPHU_PREC_FP64;
+    jo.so = so;
+    jo.want_cc = conncomp_out != nullptr;
+    jo.want_cyc = cycles_out != nullptr && in.ntr == 1 && in.ntc == 1;
+    jo.cycles_out = cycles_out;
+    return run_job(S, *params, jo, (cudaStream_t)stream, stats);
+}
+
+int cuphu_unwrap_batch_device(const CuPhuScene *scenes, int nscenes, CuPhuCostMode cost_mode,
+                              const CuPhuParams *params, const CuPhuSolveOptions *opts,
+                              CuPhuSolveStats *stats, void *stream)
+{
+    int rc = check_common(cost_mode, params);
+    if (rc) return rc;
+    if (!scenes || nscenes < 1) return fail(CUPHU_ERR_INVALID, "no scenes");
+    CuPhuSolveOptions so;
+    if (opts) so = *opts; else default_solve_options(&so);
+    std::vector<SceneIn> S(nscenes);
+    for (int i = 0; i < nscenes; ++i) {
+        const CuPhuScene &c = scenes[i];
+        if ((!c.igram_c64 && !c.phase) || !c.corr || !c.unw_out)
+            return fail(CUPHU_ERR_INVALID, "scene igram/phase, corr and unw must not be NULL");
+        if (!(c.nlooks >= 1.0)) return fail(CUPHU_ERR_INVALID, "nlooks must be >= 1");
+        SceneIn &in = S[i];
+        in.ig = reinterpret_cast<const float2 *>(c.igram_c64);
+        in.ph_in = c.igram_c64 ? nullptr : c.phase;
+        in.corr = c.corr;
+        in.mask = c.mask;
+        in.conf = c.orig_mask;
+        in.nrow = c.nrow; in.ncol = c.ncol;
+        in.ntr = c.ntilerow; in.ntc = c.ntilecol;
+        in.rovl = c.rowovrlp; in.covl = c.colovrlp;
+        in.nlooks = c.nlooks;
+        in.unw = c.unw_out;
+        in.cc = c.conncomp_out;
+        in.ref_row = so.ref_row;
+        in.ref_col = so.ref_col;
+    }
+    JobOpts jo;
+    jo.fp64 = so.precision == CUPHU_PREC_FP64;
+    jo.so = so;
+    bool cc = true;
+    for (auto &in : S) cc = cc && in.cc;
+    jo.want_cc = cc;
+    return run_job(S, *params, jo, (cudaStream_t)stream, stats);
+}
+
+int cuphu_unwrap_ex(const float *igram_c64, const float *corr, const unsigned char *mask,
+                    const unsigned char *orig_mask, int nrow, int ncol, CuPhuCostMode cost_mode,
+                    const CuPhuParams *params, const CuPhuTileParams *tile,
+                    const CuPhuSolveOptions *opts, int gpu_id, float *unw_out,
+                    uint32_t *conncomp_out, CuPhuSolveStats *stats)
+{
+    if (!igram_c64 || !corr || !unw_out || !conncomp_out)
+        return fail(CUPHU_ERR_INVALID, "igram, corr, unw and conncomp must not be NULL");
+    if (nrow < 1 || ncol < 1) return fail(CUPHU_ERR_INVALID, "nrow and ncol must be >= 1");
+    CUPHU_TRY_CUDA(cudaSetDevice(gpu_id));
+    cudaStream_t s = lib_stream(gpu_id);
+    size_t n = (size_t)nrow * ncol;
+    float *d_ig = dev_alloc_async<float>(2 * n, s), *d_corr = dev_alloc_async<float>(n, s);
+    float *d_unw = dev_alloc_async<float>(n, s);
+    uint32_t *d_cc = dev_alloc_async<uint32_t>(n, s);
+    unsigned char *d_mask = mask ? dev_alloc_async<unsigned char>(n, s) : nullptr;
+    unsigned char *d_om = orig_mask ? dev_alloc_async<unsigned char>(n, s) : nullptr;
+    int rc = 0;
+    if (!d_ig || !d_corr || !d_unw || !d_cc || (mask && !d_mask) || (orig_mask && !d_om))
+        rc = fail(CUPHU_ERR_ALLOC, "device allocation failed");
+    if (!rc) {
+        cudaMemcpyAsync(d_ig, igram_c64, 8 * n, cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(d_corr, corr, 4 * n, cudaMemcpyHostToDevice, s);
+        if (mask) cudaMemcpyAsync(d_mask, mask, n, cudaMemcpyHostToDevice, s);
+        if (orig_mask) cudaMemcpyAsync(d_om, orig_mask, n, cudaMemcpyHostToDevice, s);
+        rc = cuphu_unwrap_device(d_ig, nullptr, d_corr, d_mask, d_om, nrow, ncol, cost_mode, params,
+                                 tile, opts, d_unw, d_cc, nullptr, stats, s);
+    }
+    if (!rc) {
+        cudaMemcpyAsync(unw_out, d_unw, 4 * n, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(conncomp_out, d_cc, 4 * n, cudaMemcpyDeviceToHost, s);
+    }
+    cudaError_t e = cudaStreamSynchronize(s);
+    cudaFreeAsync(d_ig, s); cudaFreeAsync(d_corr, s); cudaFreeAsync(d_unw, s); cudaFreeAsync(d_cc, s);
+    if (d_mask) cudaFreeAsync(d_mask, s);
+    if (d_om) cudaFreeAsync(d_om, s);
+    if (!rc && e != cudaSuccess) rc = cuda_fail(e, "cuphu_unwrap_ex");
+    if (!rc) rc = device_status(gpu_id);
+    return rc;
+}
+
+int cuphu_unwrap(const float *igram_r, const float *igram_i, const float *corr, const float *mag,
+                 const unsigned char *mask, int nrow, int ncol, CuPhuCostMode cost_mode,
+                 CuPhuInitMethod init_meth, const CuPhuParams *params,
+                 const CuPhuTileParams *tile, const CuPhuBridgeParams *bridge,
+                 const unsigned char *orig_mask, int gpu_id, CuPhuResult *result)
+{
+    (void)mag;
+    if (!result) return fail(CUPHU_ERR_INVALID, "result must not be NULL");
+    result->unw = nullptr;
+    result->conncomp = nullptr;
+    result->nrow = nrow;
+    result->ncol = ncol;
+    if (init_meth != CUPHU_INIT_LAPLACE)
+        return fail(CUPHU_ERR_UNSUPPORTED,
+                    "init 'mst'/'mcf' needs SNAPHU's CPU network-flow solver, which is outside this "
+                    "build; use init 'laplace'");
+    if (bridge && bridge->enabled)
+        return fail(CUPHU_ERR_UNSUPPORTED, "phase bridging is outside this build");
+    if (!igram_r || !igram_i || !corr) return fail(CUPHU_ERR_INVALID, "igram and corr must not be NULL");
+    if (nrow < 1 || ncol < 1) return fail(CUPHU_ERR_INVALID, "nrow and ncol must be >= 1");
+    int rc = check_common(cost_mode, params);
+    if (rc) return rc;
+    if ((rc = check_tile_flags(tile))) return rc;
+    size_t n = (size_t)nrow * ncol;
+    result->unw = (float *)std::malloc(n * sizeof(float));
+    result->conncomp = (uint32_t *)std::malloc(n * sizeof(uint32_t));
+    if (!result->unw || !result->conncomp) {
+        std::free(result->unw);
+        std::free(result->conncomp);
+        result->unw = nullptr;
+        result->conncomp = nullptr;
+        return fail(CUPHU_ERR_ALLOC, "host allocation failed");
+    }
+    CUPHU_TRY_CUDA(cudaSetDevice(gpu_id));
+    cudaStream_t s = lib_stream(gpu_id);
+    float *d_re = dev_alloc_async<float>(n, s), *d_im = dev_alloc_async<float>(n, s);
+    float *d_corr = dev_alloc_async<float>(n, s), *d_unw = dev_alloc_async<float>(n, s);
+    float *d_ph = dev_alloc_async<float>(n, s);
+    uint32_t *d_cc = dev_alloc_async<uint32_t>(n, s);
+    unsigned char *d_mask = mask ? dev_alloc_async<unsigned char>(n, s) : nullptr;
+    unsigned char *d_om = orig_mask ? dev_alloc_async<unsigned char>(n, s) : nullptr;
+    if (!d_re || !d_im || !d_corr || !d_unw || !d_ph || !d_cc || (mask && !d_mask) ||
+        (orig_mask && !d_om))
+        rc = fail(CUPHU_ERR_ALLOC, "device allocation failed");
+    if (!rc) {
+        cudaMemcpyAsync(d_re, igram_r, 4 * n, cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(d_im, igram_i, 4 * n, cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(d_corr, corr, 4 * n, cudaMemcpyHostToDevice, s);
+        if (mask) cudaMemcpyAsync(d_mask, mask, n, cudaMemcpyHostToDevice, s);
+        if (orig_mask) cudaMemcpyAsync(d_om, orig_mask, n, cudaMemcpyHostToDevice, s);
+        rc = launch_phase_split(d_re, d_im, d_ph, (long long)n, s);
+    }
+    if (!rc) {
+        CuPhuSolveOptions so;
+        default_solve_options(&so);
+        CuPhuParams p = *params;
+        rc = cuphu_unwrap_device(nullptr, d_ph, d_corr, d_mask, d_om, nrow, ncol, cost_mode, &p,
+                                 tile, &so, d_unw, d_cc, nullptr, nullptr, s);
+    }
+    if (!rc) {
+        cudaMemcpyAsync(result->unw, d_unw, 4 * n, cudaMemcpyDeviceToHost, s);
+        cudaMemcpyAsync(result->conncomp, d_cc, 4 * n, cudaMemcpyDeviceToHost, s);
+    }
+    cudaError_t e = cudaStreamSynchronize(s);
+    cudaFreeAsync(d_re, s); cudaFreeAsync(d_im, s); cudaFreeAsync(d_corr, s);
+    cudaFreeAsync(d_unw, s); cudaFreeAsync(d_ph, s); cudaFreeAsync(d_cc, s);
+    if (d_mask) cudaFreeAsync(d_mask, s);
+    if (d_om) cudaFreeAsync(d_om, s);
+    if (!rc && e != cudaSuccess) rc = cuda_fail(e, "cuphu_unwrap");
+    if (!rc) rc = device_status(gpu_id);
+    return rc;
+}
+
+int cuphu_phase_gpu(const float *d_igram_c64, long long n, float *d_phase, void *stream)
+{
+    if (!d_igram_c64 || !d_phase || n < 0) return fail(CUPHU_ERR_INVALID, "bad arguments");
+    return launch_phase(reinterpret_cast<const float2 *>(d_igram_c64), d_phase, n,
+                        (cudaStream_t)stream);
+}
+
+int cuphu_residues_gpu(const float *d_phase, int nrow, int ncol, signed char *d_res, void *stream)
+{
+    if (!d_phase || !d_res || nrow < 1 || ncol < 1) return fail(CUPHU_ERR_INVALID, "bad arguments");
+    return launch_residues(d_phase, nrow, ncol, d_res, (cudaStream_t)stream);
+}
+
+int cuphu_build_costs_device(const float *d_phase, const float *d_corr, const short *d_weights,
+                             int nrow, int ncol, int mode, const CuPhuParams *params,
+                             void *d_costs, signed char *d_residues, void *stream)
+{
+    int rc = check_common((CuPhuCostMode)mode, params);
+    if (rc) return rc;
+    if (!d_phase || !d_corr || !d_costs || nrow < 1 || ncol < 1)
+        return fail(CUPHU_ERR_INVALID, "bad arguments");
+    return launch_costs(d_phase, d_corr, d_weights, nrow, ncol, mode, *params, d_costs, d_residues,
+                        (cudaStream_t)stream);
+}
+
+static int build_costs_launcher(const float *d_phase, const float *d_corr, const short *d_roww,
+                                const short *d_colw, int nrow, int ncol, const CuPhuParams *params,
+                                int kperp, int kpar, void **d_costs_out, void *stream, int mode)
+{
+    if (!d_costs_out) return fail(CUPHU_ERR_INVALID, "d_costs_out must not be NULL");
+    *d_costs_out = nullptr;
+    if (!params || !d_phase || !d_corr || nrow < 1 || ncol < 1)
+        return fail(CUPHU_ERR_INVALID, "bad arguments");
+    if ((d_roww == nullptr) != (d_colw == nullptr))
+        return fail(CUPHU_ERR_INVALID, "row and column weights must both be given or both NULL");
+    cudaStream_t s = (cudaStream_t)stream;
+    size_t nra = (size_t)(nrow - 1) * ncol, nca = (size_t)nrow * (ncol - 1);
+    size_t es = mode ? 8 : 4;
+    void *out = nullptr;
+    CUPHU_TRY_CUDA(cudaMallocAsync(&out, (nra + nca) * es + 8, s));
+    short *w = nullptr;
+    if (d_roww) {
+        /* the launcher interface passes two weight arrays; the kernel reads
+         * one flat array, so gather them once */
+        CUPHU_TRY_CUDA(cudaMallocAsync((void **)&w, (nra + nca) * sizeof(short) + 8, s));
+        CUPHU_TRY_CUDA(cudaMemcpyAsync(w, d_roww, nra * sizeof(short), cudaMemcpyDeviceToDevice, s));
+        CUPHU_TRY_CUDA(cudaMemcpyAsync(w + nra, d_colw, nca * sizeof(short), cudaMemcpyDeviceToDevice, s));
+    }
+    CuPhuParams p = *params;
+    p.kperpdpsi = kperp;
+    p.kpardpsi = kpar;
+    int rc = launch_costs(d_phase, d_corr, w, nrow, ncol, mode, p, out, nullptr, s);
+    if (w) cudaFreeAsync(w, s);
+    if (rc) {
+        cudaFreeAsync(out, s);
+        return rc;
+    }
+    *d_costs_out = out;
+    return 0;
+}
+
+int cuphu_build_smooth_costs_gpu(const float *d_phase, const float *d_corr, const short *d_roww,
+                                 const short *d_colw, int nrow, int ncol,
+                                 const CuPhuParams *params, int kperpdpsi, int kpardpsi,
+                                 void **d_costs_out, void *stream)
+{
+    return build_costs_launcher(d_phase, d_corr, d_roww, d_colw, nrow, ncol, params, kperpdpsi,
+                                kpardpsi, d_costs_out, stream, 0);
+}
+
+int cuphu_build_defo_costs_gpu(const float *d_phase, const float *d_corr, const short *d_roww,
+                               const short *d_colw, int nrow, int ncol, const CuPhuParams *params,
+                               int kperpdpsi, int kpardpsi, void **d_costs_out, void *stream)
+{
+    return build_costs_launcher(d_phase, d_corr, d_roww, d_colw, nrow, ncol, params, kperpdpsi,
+                                kpardpsi, d_costs_out, stream, 1);
+}
+
+int cuphu_build_costs_gpu(const float *igram_r, const float *igram_i, const float *corr,
+                          const float *mag, const short *weights, int nrow, int ncol,
+                          CuPhuCostMode cost_mode, const CuPhuParams *params, int gpu_id,
+                          void **costs_out, size_t *cost_elem_sz)
+{
+    (void)mag;
+    if (!costs_out || !cost_elem_sz) return fail(CUPHU_ERR_INVALID, "output pointers must not be NULL");
+    *costs_out = nullptr;
+    *cost_elem_sz = 0;
+    int rc = check_common(cost_mode, params);
+    if (rc) return rc;
+    if (!igram_r || !igram_i || !corr || nrow < 1 || ncol < 1)
+        return fail(CUPHU_ERR_INVALID, "bad arguments");
+    CUPHU_TRY_CUDA(cudaSetDevice(gpu_id));
+    cudaStream_t s = lib_stream(gpu_id);
+    size_t n = (size_t)nrow * ncol;
+    size_t narcs = (size_t)(nrow - 1) * ncol + (size_t)nrow * (ncol - 1);
+    size_t es = cost_mode == CUPHU_COST_SMOOTH ? 4 : 8;
+    float *d_re = dev_alloc_async<float>(n, s), *d_im = dev_alloc_async<float>(n, s);
+    float *d_corr = dev_alloc_async<float>(n, s), *d_ph = dev_alloc_async<float>(n, s);
+    short *d_w = weights ? dev_alloc_async<short>(narcs, s) : nullptr;
+    char *d_c = dev_alloc_async<char>(narcs * es + 8, s);
+    void *h = std::malloc(narcs * es + 8);
+    if (!d_re || !d_im || !d_corr || !d_ph || !d_c || (weights && !d_w) || !h)
+        rc = fail(CUPHU_ERR_ALLOC, "allocation failed");
+    if (!rc) {
+        cudaMemcpyAsync(d_re, igram_r, 4 * n, cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(d_im, igram_i, 4 * n, cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(d_corr, corr, 4 * n, cudaMemcpyHostToDevice, s);
+        if (weights) cudaMemcpyAsync(d_w, weights, 2 * narcs, cudaMemcpyHostToDevice, s);
+        rc = launch_phase_split(d_re, d_im, d_ph, (long long)n, s);
+    }
+    if (!rc)
+        rc = launch_costs(d_ph, d_corr, d_w, nrow, ncol, cost_mode == CUPHU_COST_SMOOTH ? 0 : 1,
+                          *params, d_c, nullptr, s);
+    if (!rc) cudaMemcpyAsync(h, d_c, narcs * es, cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    cudaFreeAsync(d_re, s); cudaFreeAsync(d_im, s); cudaFreeAsync(d_corr, s);
+    cudaFreeAsync(d_ph, s); cudaFreeAsync(d_c, s);
+    if (d_w) cudaFreeAsync(d_w, s);
+    if (!rc && e != cudaSuccess) rc = cuda_fail(e, "cuphu_build_costs_gpu");
+    if (rc) {
+        std::free(h);
+        return rc;
+    }
+    *costs_out = h;
+    *cost_elem_sz = es;
+    return (int)es;
+}
+
+int cuphu_laplace_solve_device(const void *d_costs, int cost_stride_shorts, const float *d_phase,
+                               int nrow, int ncol, const CuPhuSolveOptions *opts, float *d_unw,
+                               int32_t *d_cycles, float *d_cont, CuPhuSolveStats *stats,
+                               void *stream)
+{
+    if (!d_costs || !d_phase || !d_unw || nrow < 1 || ncol < 1)
+        return fail(CUPHU_ERR_INVALID, "bad arguments");
+    if (cost_stride_shorts != 2 && cost_stride_shorts != 4)
+        return fail(CUPHU_ERR_INVALID, "cost stride must be 2 (smooth) or 4 (defo) shorts");
+    CuPhuParams p;
+    cuphu_default_params(&p);
+    CuPhuSolveOptions so;
+    if (opts) so = *opts; else default_solve_options(&so);
+    SceneIn in;
+    in.ph_in = d_phase;
+    in.corr = d_phase;   /* not read: weights come from the cost array */
+    in.nrow = nrow;
+    in.ncol = ncol;
+    in.unw = d_unw;
+    in.nlooks = p.ncorrlooks;
+    in.ref_row = so.ref_row;
+    in.ref_col = so.ref_col;
+    std::vector<SceneIn> S(1, in);
+    JobOpts jo;
+    jo.fp64 = so.precision == CUPHU_PREC_FP64;
+    jo.so = so;
+    jo.want_cc = false;
+    jo.want_cyc = d_cycles != nullptr;
+    jo.cycles_out = d_cycles;
+    jo.costs = (const short *)d_costs;
+    jo.cost_stride = cost_stride_shorts;
+    jo.cont_out = d_cont;
+    return run_job(S, p, jo, (cudaStream_t)stream, stats);
+}
+
+int cuphu_laplace_unwrap_gpu(const void *d_smooth_costs, const float *d_phase, int nrow, int ncol,
+                             double nshortcycle, int max_iter, float tol, int verbose, float *d_unw,
+                             void *stream)
+{
+    (void)nshortcycle;
+    (void)verbose;
+    CuPhuSolveOptions so;
+    default_solve_options(&so);
+    so.max_iter = max_iter;
+    so.tol = tol;
+    return cuphu_laplace_solve_device(d_smooth_costs, 2, d_phase, nrow, ncol, &so, d_unw, nullptr,
+                                      nullptr, nullptr, stream);
+}
+
+int cuphu_integrate_phase_gpu(const float *wrapped_phase, const short *hflows, const short *vflows,
+                              int nrow, int ncol, int gpu_id, float *unw_out)
+{
+    if (!wrapped_phase || !hflows || !vflows || !unw_out || nrow < 1 || ncol < 1)
+        return fail(CUPHU_ERR_INVALID, "bad arguments");
+    CUPHU_TRY_CUDA(cudaSetDevice(gpu_id));
+    cudaStream_t s = lib_stream(gpu_id);
+    float *rowoff = dev_alloc_async<float>(nrow, s);
+    if (!rowoff) return fail(CUPHU_ERR_ALLOC, "device allocation failed");
+    int rc = launch_integrate(wrapped_phase, hflows, vflows, nrow, ncol, rowoff, unw_out, s);
+    cudaFreeAsync(rowoff, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (!rc && e != cudaSuccess) rc = cuda_fail(e, "cuphu_integrate_phase_gpu");
+    return rc;
+}
+
+static int conncomp_scene(const float *unw, const float *corr, const unsigned char *mask, int nrow,
+                          int ncol, const short *poscost, const short *negcost, float corr_thresh,
+                          long conncompthresh, double minfrac, long maxncomps, uint32_t *labels_out,
+                          cudaStream_t s)
+{
+    TileDesc T = {};
+    T.ph = unw;
+    T.corr = corr;
+    T.mask = mask;
+    T.ph_pitch = ncol;
+    T.nr = nrow;
+    T.nc = ncol;
+    T.pitch = (ncol + 3) & ~3;
+    T.nbx = (ncol + kItemBx - 1) / kItemBx;
+    T.nitems = T.nbx * ((nrow + kItemBy - 1) / kItemBy);
+    size_t np = (size_t)nrow * T.pitch;
+    char *buf = dev_alloc_async<char>(np * 12 + sizeof(TileDesc) + (size_t)T.nitems * 4 +
+                                          (size_t)nrow * 8 + 4096, s);
+    if (!buf) return fail(CUPHU_ERR_ALLOC, "device allocation failed");
+    Bump b(buf);
+    SolverPlanes P = {};
+    P.unw = b.take<float>(np);
+    P.cc = b.take<uint32_t>(np);
+    P.aux = b.take<uint32_t>(np);
+    TileDesc *d_t = b.take<TileDesc>(1);
+    int *d_item = b.take<int>(T.nitems);
+    int *d_row = b.take<int>(2 * (size_t)nrow);
+    int *d_nlab = b.take<int>(1);
+    std::vector<int> zeros(std::max(T.nitems, nrow), 0);
+    int rc = 0;
+    cudaMemcpyAsync(d_t, &T, sizeof(T), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_item, zeros.data(), T.nitems * 4, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_row + nrow, zeros.data(), (size_t)nrow * 4, cudaMemcpyHostToDevice, s);
+    cudaMemcpy2DAsync(P.unw, (size_t)T.pitch * 4, unw, (size_t)ncol * 4, (size_t)ncol * 4, nrow,
+                      cudaMemcpyDeviceToDevice, s);
+    CcArgs ca;
+    ca.poscost = poscost;
+    ca.negcost = negcost;
+    ca.corr_thresh = corr_thresh;
+    ca.conncompthresh = conncompthresh;
+    ca.minfrac = minfrac;
+    ca.maxncomps = (int)std::min<long>(maxncomps, 0x7fffffffL);
+    rc = launch_conncomp(d_t, 1, nrow, d_item, T.nitems, P, ca, d_row, d_nlab, s);
+    if (!rc)
+        cudaMemcpy2DAsync(labels_out, (size_t)ncol * 4, P.cc, (size_t)T.pitch * 4, (size_t)ncol * 4,
+                          nrow, cudaMemcpyDeviceToDevice, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    cudaFreeAsync(buf, s);
+    cudaStreamSynchronize(s);
+    if (!rc && e != cudaSuccess) rc = cuda_fail(e, "conncomp");
+    return rc;
+}
+
+int cuphu_conncomp_gpu(const float *unw, const float *corr, const unsigned char *mask, int nrow,
+                       int ncol, const short *poscost, const short *negcost,
+                       const CuPhuParams *params, int gpu_id, uint32_t *labels_out)
+{
+    if (!unw || !corr || !labels_out || !params || nrow < 1 || ncol < 1)
+        return fail(CUPHU_ERR_INVALID, "bad arguments");
+    if ((poscost == nullptr) != (negcost == nullptr))
+        return fail(CUPHU_ERR_INVALID, "poscost and negcost must both be given or both NULL");
+    CUPHU_TRY_CUDA(cudaSetDevice(gpu_id));
+    return conncomp_scene(unw, corr, mask, nrow, ncol, poscost, negcost, 0.05f,
+                          params->conncompthresh, params->minconncompfrac, params->maxncomps,
+                          labels_out, lib_stream(gpu_id));
+}
+
+int cuphu_conncomp_ex(const float *unw, const float *corr, const unsigned char *mask, int nrow,
+                      int ncol, float corr_thresh, double minfrac, long maxncomps, int gpu_id,
+                      uint32_t *labels_out)
+{
+    if (!unw || !corr || !labels_out || nrow < 1 || ncol < 1)
+        return fail(CUPHU_ERR_INVALID, "bad arguments");
+    CUPHU_TRY_CUDA(cudaSetDevice(gpu_id));
+    cudaStream_t s = lib_stream(gpu_id);
+    size_t n = (size_t)nrow * ncol;
+    float *du = dev_alloc_async<float>(n, s), *dc = dev_alloc_async<float>(n, s);
+    unsigned char *dm = mask ? dev_alloc_async<unsigned char>(n, s) : nullptr;
+    uint32_t *dl = dev_alloc_async<uint32_t>(n, s);
+    int rc = 0;
+    if (!du || !dc || !dl || (mask && !dm)) rc = fail(CUPHU_ERR_ALLOC, "device allocation failed");
+    if (!rc) {
+        cudaMemcpyAsync(du, unw, 4 * n, cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(dc, corr, 4 * n, cudaMemcpyHostToDevice, s);
+        if (mask) cudaMemcpyAsync(dm, mask, n, cudaMemcpyHostToDevice, s);
+        rc = conncomp_scene(du, dc, dm, nrow, ncol, nullptr, nullptr, corr_thresh, 0, minfrac,
+                            maxncomps, dl, s);
+    }
+    if (!rc) cudaMemcpyAsync(labels_out, dl, 4 * n, cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    cudaFreeAsync(du, s); cudaFreeAsync(dc, s); cudaFreeAsync(dl, s);
+    if (dm) cudaFreeAsync(dm, s);
+    if (!rc && e != cudaSuccess) rc = cuda_fail(e, "cuphu_conncomp_ex");
+    return rc;
+}
+
+int cuphu_incrcost_early_exit(const void *d_costs_flat, const short *d_flows_flat, int narcs,
+                              long nshortcycle, int nflow, short *d_poscost, short *d_negcost,
+                              int *d_scratch)
+{
+    if (!d_costs_flat || !d_flows_flat || !d_poscost || !d_negcost || !d_scratch || narcs < 0)
+        return fail(CUPHU_ERR_INVALID, "bad arguments");
+    if (nflow < 1) return fail(CUPHU_ERR_INVALID, "nflow must be >= 1");
+    int rc = launch_incrcost((const short *)d_costs_flat, d_flows_flat, narcs, nshortcycle, nflow,
+                             d_poscost, d_negcost, d_scratch, 0);
+    if (rc) return rc;
+    int h[2];
+    CUPHU_TRY_CUDA(cudaMemcpy(h, d_scratch, sizeof(h), cudaMemcpyDeviceToHost));
+    return (h[0] >= 0 && h[1] >= 0) ? 1 : 0;
+}
+
+int cuphu_gpu_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+int cuphu_gpu_name(int device, char *buf, int len)
+{
+    cudaDeviceProp p;
+    CUPHU_TRY_CUDA(cudaGetDeviceProperties(&p, device));
+    if (buf && len > 0) {
+        std::strncpy(buf, p.name, (size_t)len - 1);
+        buf[len - 1] = 0;
+    }
+    return 0;
+}
+
+int cuphu_gpu_info(int device, long long *total_memory, int *sm_count, int *cc_major, int *cc_minor)
+{
+    cudaDeviceProp p;
+    CUPHU_TRY_CUDA(cudaGetDeviceProperties(&p, device));
+    if (total_memory) *total_memory = (long long)p.totalGlobalMem;
+    if (sm_count) *sm_count = p.multiProcessorCount;
+    if (cc_major) *cc_major = p.major;
+    if (cc_minor) *cc_minor = p.minor;
+    return 0;
+}
+
+int cuphu_last_status(int gpu_id)
+{
+    if (gpu_id < 0 || gpu_id >= 64) return fail(CUPHU_ERR_INVALID, "device index out of range");
+    return device_status(gpu_id);
+}
+
+int cuphu_release_workspace(int gpu_id)
+{
+    if (gpu_id < 0 || gpu_id >= 64) return fail(CUPHU_ERR_INVALID, "device index out of range");
+    Workspace &W = g_ws[gpu_id];
+    std::lock_guard<std::mutex> lock(W.mu);
+    CUPHU_TRY_CUDA(cudaSetDevice(gpu_id));
+    CUPHU_TRY_CUDA(cudaDeviceSynchronize());
+    if (W.dev) cudaFree(W.dev);
+    if (W.host) cudaFreeHost(W.host);
+    W.dev = nullptr;
+    W.host = nullptr;
+    W.dev_size = W.host_size = 0;
+    return 0;
+}
+
+}  /* extern "C" */

@@ -1,0 +1,135 @@
+/*
+ * kernels.cuh -- device data structures shared by the kernels and the host
+ * orchestrator, and the launcher declarations.
+ *
+ * HBM layout: every tile of every scene owns a slab of pitched planes
+ * (pitch = ncol rounded up to 4 elements, so every row starts 16-byte
+ * aligned for vector loads).  Arc weights live in two planes: wd[r][c] is
+ * the down arc (r,c)->(r+1,c) (the reference's row arc, cuphu_laplace.cu:85)
+ * and wr[r][c] the right arc (r,c)->(r,c+1) (col arc, :86); the last row of
+ * wd and the last column of wr are zero.  Scene-level arrays (phase, corr,
+ * mask, outputs) stay in the caller's row-major layout and tiles address them
+ * through origin pointers.
+ */
+#pragma once
+
+#include "common.cuh"
+
+namespace cuphu {
+
+struct TileDesc {
+    const float *ph;            /* wrapped phase at the tile origin (scene layout) */
+    const float *corr;          /* coherence at the tile origin                    */
+    const unsigned char *mask;  /* solve mask at the tile origin, or NULL          */
+    const unsigned char *conf;  /* stitching confidence mask, or NULL              */
+    int ph_pitch;               /* scene row pitch (ncol)                          */
+    int scene;
+    int nr, nc, pitch;          /* tile shape and plane pitch                      */
+    int r0, c0;                 /* origin in the scene                             */
+    int tr, tc;                 /* position in the scene's tile grid               */
+    long long pix;              /* plane offset of this tile (elements)            */
+    int item0, nbx, nitems;     /* solver work items                               */
+    int row0;                   /* offset of this tile's rows in per-row arrays   */
+};
+
+struct SolverPlanes {
+    float *w0d, *w0r;           /* data weights 1/sigsq                  */
+    float *wd, *wr;             /* current IRLS weights                  */
+    void *x, *r, *p0, *p1;      /* PCG state, float or double; p is     */
+    void *q, *diag;             /* double-buffered across iterations     */
+    float *unw;                 /* congruent unwrapped phase per tile    */
+    int32_t *cyc;               /* optional cycle map per tile           */
+    float *cont;                /* optional anchored continuous solution */
+    uint32_t *cc;               /* union-find parents, then labels       */
+    uint32_t *aux;              /* component sizes, then root labels     */
+};
+
+struct TileState {
+    double rz, rz0, thr, alpha, beta;
+    int active, iter, pad0, pad1;
+    unsigned ticket, pad2;
+};
+
+struct SolverCtl {
+    unsigned bar_count, bar_gen;
+    int err, n_active, snap;
+    int total_iters, max_pass_iters, pad;
+};
+
+struct SolveParams {
+    int n_irls, max_iter, replace_every;
+    float tol;
+    const float *deltas;        /* per-pass IRLS delta (host powf schedule) */
+    int *pass_iters;            /* [n_irls+1] iterations per pass (out)     */
+    long long timeout_ns;       /* grid-barrier wait limit                   */
+};
+
+struct ScenePlan {
+    float *unw_out;
+    uint32_t *cc_out;
+    const float *ph;            /* scene wrapped phase */
+    int nrow, ncol;
+    int ntr, ntc, rovl, covl;
+    int tile0;                  /* first tile index */
+    int pair0;                  /* first stitching pair (horizontal then vertical) */
+    const int *rowmap, *colmap; /* merge maps: scene row/col -> tile row/col */
+    int ref_row, ref_col;
+    int maxncomps;
+    double minfrac;
+    int single;
+};
+
+struct PairDesc {
+    int a, b, dir;              /* tiles; dir 0 = a left of b, 1 = a above b */
+    int ov;
+};
+
+struct SceneOut {               /* filled by k_stitch_finalize */
+    float shift;
+    int do_shift;
+};
+
+/* cost.cu */
+int launch_phase(const float2 *ig, float *ph, long long n, cudaStream_t s);
+int launch_phase_split(const float *re, const float *im, float *ph, long long n, cudaStream_t s);
+int launch_costs(const float *ph, const float *corr, const short *weights, int nrow, int ncol,
+                 int mode, const CuPhuParams &p, void *costs, signed char *res, cudaStream_t s);
+int launch_residues(const float *ph, int nrow, int ncol, signed char *res, cudaStream_t s);
+int launch_w0(const TileDesc *tiles, const int *item_tile, int nitems, const CostConsts *sk,
+              const SolverPlanes &P, cudaStream_t s);
+int launch_w0_from_costs(const short *costs, int stride, int nrow, int ncol, int pitch,
+                         const SolverPlanes &P, cudaStream_t s);
+
+/* laplace.cu */
+int launch_solve(bool fp64, const TileDesc *tiles, const int *item_tile, int nitems,
+                 int ntiles, const SolverPlanes &P, TileState *st, double *part,
+                 SolverCtl *ctl, const SolveParams &sp, int device, cudaStream_t s);
+
+/* conncomp.cu */
+struct CcArgs {
+    const short *poscost, *negcost;   /* flat arc layout of a single scene, or NULL */
+    float corr_thresh;                /* validity floor, 0.05 (cuphu_conncomp.cu:324-325) */
+    long conncompthresh;
+    double minfrac;
+    int maxncomps;
+};
+int launch_conncomp(const TileDesc *tiles, int ntiles, int total_rows, const int *item_tile,
+                    int nitems, const SolverPlanes &P, const CcArgs &a, int *rowcnt,
+                    int *ntile_labels, cudaStream_t s);
+
+/* stitch.cu */
+int launch_stitch(const ScenePlan *scenes, int nscenes, const TileDesc *tiles,
+                  const PairDesc *pairs, int npairs, const SolverPlanes &P,
+                  const int *ntile_labels, double *pair_k, double *tile_k,
+                  unsigned *comp_off, SceneOut *sout, cudaStream_t s);
+int launch_merge(const ScenePlan *scenes, const ScenePlan *h_scenes, int nscenes,
+                 const TileDesc *tiles, const SolverPlanes &P, const double *tile_k,
+                 const unsigned *comp_off, const SceneOut *sout, cudaStream_t s);
+
+/* integrate.cu */
+int launch_integrate(const float *ph, const short *hflows, const short *vflows, int nrow,
+                     int ncol, float *rowoff, float *unw, cudaStream_t s);
+int launch_incrcost(const short *costs, const short *flows, int narcs, long nsc, int nflow,
+                    short *pos, short *neg, int *scratch, cudaStream_t s);
+
+}  // namespace cuphu

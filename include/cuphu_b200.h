@@ -1,0 +1,297 @@
+/*
+ * cuphu_b200.h -- C ABI of the B200-native cuPHU unwrapping path.
+ *
+ * Drop-in for the reference's C interface (src/cxx/cuphu/cuphu.h).  Structs
+ * and enums keep the reference's field order and values so a caller built
+ * against the reference header links against libcuphu_b200.so unchanged.
+ * Every entry point returns an int status (0 = success, negative =
+ * cuphu_status_t) instead of throwing across the ABI (the reference throws
+ * std::runtime_error from CUDA_CHECK, cuphu.h:432-440); the message of the
+ * last failure on the calling thread is available from cuphu_last_error().
+ *
+ * Streams are passed as void* (a cudaStream_t; NULL = legacy default stream).
+ * "Device" pointers must be device-accessible memory on the selected GPU.
+ */
+#ifndef CUPHU_B200_H
+#define CUPHU_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ── status codes (new; the reference throws instead) ──────────────────── */
+typedef enum {
+    CUPHU_OK                 =  0,
+    CUPHU_ERR_ALLOC          = -1,  /* host or device allocation failed (ref: -1) */
+    CUPHU_ERR_INVALID        = -2,  /* bad argument (shape, pointer, mode)         */
+    CUPHU_ERR_CUDA           = -3,  /* CUDA runtime error                          */
+    CUPHU_ERR_UNSUPPORTED    = -4,  /* feature outside this build (MCF/MST, bridge)*/
+    CUPHU_ERR_TIMEOUT        = -5,  /* a device-side wait hit its spin limit       */
+    CUPHU_ERR_NOT_CONVERGED  = -6   /* reserved: a loop hit its iteration cap      */
+} cuphu_status_t;
+
+/* ref cuphu.h:19-23 */
+typedef enum {
+    CUPHU_COST_SMOOTH = 0,
+    CUPHU_COST_DEFO   = 1,
+    CUPHU_COST_TOPO   = 2
+} CuPhuCostMode;
+
+/* ref cuphu.h:26-30 */
+typedef enum {
+    CUPHU_INIT_MST     = 0,
+    CUPHU_INIT_MCF     = 1,
+    CUPHU_INIT_LAPLACE = 2
+} CuPhuInitMethod;
+
+/* ref cuphu.h:33-92 -- identical layout */
+typedef struct CuPhuParams {
+    double nlooks, ncorrlooks, defothreshfactor, rhosconst1, rhosconst2;
+    double cstd1, cstd2, cstd3;
+    double sigsqcorr, costscale, nshortcycle;
+    long   sigsqshortmin;
+    double orbitradius, altitude, earthradius, baseline, baselineangle, bperp;
+    int    transmitmode;
+    long   nlooksrange, nlooksaz, nlooksother, ncorrlooksrange, ncorrlooksaz;
+    double nearrange, dr, da, rangeres, azres, lambda;
+    double kds, specularexp, dzrcritfactor;
+    int    shadow;
+    double dzeimin;
+    long   laywidth;
+    double layminei, sloperatiofactor, sigsqei;
+    double dzlaypeak, azdzfactor, dzeifactor, dzeiweight;
+    double dzlayfactor, layconst, layfalloffconst, sigsqlayfactor;
+    double defoazdzfactor, defomax, defolayconst;
+    int    kperpdpsi, kpardpsi;
+    double p, maxcost, costscaleambight, dnomincangle;
+    double initdzr, initdzstep, threshold;
+    long   initmaxflow, arcmaxflowconst, maxflow, nshortcycleL;
+    long   cs2scalefactor;
+    double minconncompfrac;
+    long   conncompthresh;
+    long   maxncomps;
+} CuPhuParams;
+
+/* ref cuphu.h:95-138 -- identical layout */
+typedef struct CuPhuTileParams {
+    int ntilerow, ntilecol;
+    int rowovrlp, colovrlp;
+    int tilecostthresh;
+    int minregionsize;
+    int nproc;
+    int ngpustreams;
+    int single_tile_reoptimize;
+    int laplace_neighbor_feedback;
+    int laplace_neighbor_feedback_feather;
+    int fix_cycle_spikes;
+} CuPhuTileParams;
+
+/* ref cuphu.h:142-162 -- identical layout; bridging is not part of this
+ * build, enabled != 0 returns CUPHU_ERR_UNSUPPORTED */
+typedef enum {
+    CUPHU_RAMP_NONE = 0, CUPHU_RAMP_LINEAR, CUPHU_RAMP_QUADRATIC,
+    CUPHU_RAMP_LINEAR_RANGE, CUPHU_RAMP_LINEAR_AZIMUTH,
+    CUPHU_RAMP_QUADRATIC_RANGE, CUPHU_RAMP_QUADRATIC_AZIMUTH
+} CuPhuRampType;
+
+typedef struct CuPhuBridgeParams {
+    int enabled, radius, min_num_pixel, erosion_size, max_boundary_samples;
+    CuPhuRampType ramp_type;
+    int ramp_max_num_sample;
+} CuPhuBridgeParams;
+
+/* ref cuphu.h:165-169; unw/conncomp are malloc'd by the callee, caller frees */
+typedef struct CuPhuResult {
+    float    *unw;
+    uint32_t *conncomp;
+    int       nrow, ncol;
+} CuPhuResult;
+
+/* ── solver options (new; no reference counterpart -- the reference reads
+ *    the same knobs from CUPHU_N_IRLS, CUPHU_IRLS_DELTA_MAX/MIN,
+ *    CUPHU_LAPLACE_MAX_ITER and CUPHU_LAPLACE_TOL, cuphu_laplace.cu:385-390
+ *    and cuphu_solver.cpp:468-472, which cuphu_default_solve_options honours) */
+typedef enum {
+    CUPHU_PREC_MIXED = 0,   /* FP32 stencil/vectors, FP64 dots + residual replacement */
+    CUPHU_PREC_FP64  = 1    /* FP64 vectors and dots ("plain FP64 PCG")              */
+} CuPhuPrecision;
+
+typedef struct CuPhuSolveOptions {
+    int   precision;          /* CuPhuPrecision                                  */
+    int   n_irls;             /* IRLS re-solves after the first (default 16)     */
+    float irls_delta_max;     /* 0.5                                             */
+    float irls_delta_min;     /* 0.01                                            */
+    int   max_iter;           /* PCG matvecs per solve (1000)                    */
+    float tol;                /* stop when rz < tol^2 rz0 (1e-3)                 */
+    int   replace_every;      /* mixed: true-residual replacement period (50)    */
+    int   ref_row, ref_col;   /* reference pixel; -1 disables the 2pi shift      */
+    int   timeout_ms;         /* device spin limit per grid barrier (5000)       */
+} CuPhuSolveOptions;
+
+/* per-call statistics (new) */
+typedef struct CuPhuSolveStats {
+    int    ntiles;
+    int    total_iters;       /* sum over passes of the max PCG iterations      */
+    int    max_iters_pass;    /* largest per-pass iteration count                */
+    double solve_ms;          /* device time of the persistent solve            */
+    double total_ms;          /* device time of the whole GPU pipeline          */
+} CuPhuSolveStats;
+
+/* ── defaults (ref cuphu.h:177-179) ─────────────────────────────────────── */
+void cuphu_default_params(CuPhuParams *p);
+void cuphu_default_tile_params(CuPhuTileParams *tp);
+void cuphu_default_bridge_params(CuPhuBridgeParams *bp);
+void cuphu_default_solve_options(CuPhuSolveOptions *o);          /* new */
+
+const char *cuphu_last_error(void);                               /* new */
+
+/* ── full pipeline (ref cuphu.h:218-234, cuphu_solver.cpp:1675) ─────────────
+ * Host pointers.  init_meth must be CUPHU_INIT_LAPLACE; MST/MCF need SNAPHU's
+ * CPU network-flow solver, which is outside this build
+ * (CUPHU_ERR_UNSUPPORTED).  mag is accepted and unused, as in the
+ * reference's Laplace branch. */
+int cuphu_unwrap(const float *igram_r, const float *igram_i, const float *corr,
+                 const float *mag, const unsigned char *mask, int nrow, int ncol,
+                 CuPhuCostMode cost_mode, CuPhuInitMethod init_meth,
+                 const CuPhuParams *params, const CuPhuTileParams *tile,
+                 const CuPhuBridgeParams *bridge, const unsigned char *orig_mask,
+                 int gpu_id, CuPhuResult *result);
+
+/* new: interleaved complex64 igram, caller-owned outputs, solver options and
+ * statistics.  Host pointers; igram = 2*nrow*ncol floats (re, im). */
+int cuphu_unwrap_ex(const float *igram_c64, const float *corr, const unsigned char *mask,
+                    const unsigned char *orig_mask, int nrow, int ncol,
+                    CuPhuCostMode cost_mode, const CuPhuParams *params,
+                    const CuPhuTileParams *tile, const CuPhuSolveOptions *opts,
+                    int gpu_id, float *unw_out, uint32_t *conncomp_out,
+                    CuPhuSolveStats *stats);
+
+/* new: the same pipeline on device-resident data, asynchronous on `stream`
+ * (returns after enqueueing; stats are filled after a stream sync inside
+ * the call only when stats != NULL).  phase_in may replace igram_c64: when
+ * igram_c64 is NULL the wrapped phase (radians) is read from phase_in.  The
+ * optional cycles_out receives the integer cycle map k (int32, nrow*ncol) with
+ * unw = phi + 2*pi*k before tile stitching and the reference-pixel shift
+ * (single-tile scenes only; NULL otherwise). */
+int cuphu_unwrap_device(const float *igram_c64, const float *phase_in, const float *corr,
+                        const unsigned char *mask, const unsigned char *orig_mask,
+                        int nrow, int ncol, CuPhuCostMode cost_mode,
+                        const CuPhuParams *params, const CuPhuTileParams *tile,
+                        const CuPhuSolveOptions *opts, float *unw_out,
+                        uint32_t *conncomp_out, int32_t *cycles_out,
+                        CuPhuSolveStats *stats, void *stream);
+
+/* new: batched solve of many independent scenes in one persistent launch
+ * (device pointers; tiles of every scene share one solver launch). */
+typedef struct CuPhuScene {
+    const float         *igram_c64;   /* device, or NULL with phase      */
+    const float         *phase;       /* device wrapped phase, or NULL   */
+    const float         *corr;        /* device                          */
+    const unsigned char *mask;        /* device or NULL                  */
+    const unsigned char *orig_mask;   /* device or NULL                  */
+    int                  nrow, ncol;
+    int                  ntilerow, ntilecol, rowovrlp, colovrlp;
+    double               nlooks;
+    float               *unw_out;     /* device                          */
+    uint32_t            *conncomp_out;/* device                          */
+} CuPhuScene;
+
+int cuphu_unwrap_batch_device(const CuPhuScene *scenes, int nscenes,
+                              CuPhuCostMode cost_mode, const CuPhuParams *params,
+                              const CuPhuSolveOptions *opts, CuPhuSolveStats *stats,
+                              void *stream);
+
+/* ── cost build (ref cuphu.h:243-256, cuphu_solver.cpp:2104-2171) ─────────
+ * Host pointers.  Returns the element size (4 smooth, 8 defo/topo) or a
+ * negative status; *costs_out is malloc'd (row arcs then col arcs). */
+int cuphu_build_costs_gpu(const float *igram_r, const float *igram_i, const float *corr,
+                          const float *mag, const short *weights, int nrow, int ncol,
+                          CuPhuCostMode cost_mode, const CuPhuParams *params, int gpu_id,
+                          void **costs_out, size_t *cost_elem_sz);
+
+/* launcher level, device pointers (ref cuphu_cost.cu:339-411, 418-479).
+ * *d_costs_out is allocated with cudaMallocAsync on `stream`; free it with
+ * cudaFree / cudaFreeAsync.  d_roww/d_colw may be NULL (all weights 1). */
+int cuphu_build_smooth_costs_gpu(const float *d_phase, const float *d_corr,
+                                 const short *d_roww, const short *d_colw, int nrow, int ncol,
+                                 const CuPhuParams *params, int kperpdpsi, int kpardpsi,
+                                 void **d_costs_out, void *stream);
+int cuphu_build_defo_costs_gpu(const float *d_phase, const float *d_corr,
+                               const short *d_roww, const short *d_colw, int nrow, int ncol,
+                               const CuPhuParams *params, int kperpdpsi, int kpardpsi,
+                               void **d_costs_out, void *stream);
+
+/* new: costs into a caller buffer (device), optional residues
+ * ((nrow-1)*(ncol-1) int8, device or NULL).  mode: CuPhuCostMode. */
+int cuphu_build_costs_device(const float *d_phase, const float *d_corr,
+                             const short *d_weights, int nrow, int ncol, int mode,
+                             const CuPhuParams *params, void *d_costs,
+                             signed char *d_residues, void *stream);
+
+/* new: residues of a wrapped phase (device; (nrow-1)*(ncol-1) int8) */
+int cuphu_residues_gpu(const float *d_phase, int nrow, int ncol, signed char *d_res,
+                       void *stream);
+
+/* new: wrapped phase in [0,2pi) from an interleaved complex64 igram (device) */
+int cuphu_phase_gpu(const float *d_igram_c64, long long n, float *d_phase, void *stream);
+
+/* ── Laplace solve, launcher level (ref cuphu_laplace.cu:352-552) ─────────
+ * d_smooth_costs: smoothcostT (offset, sigsq int16 pairs) in the flat
+ * row-then-col layout; d_phase wrapped phase; d_unw output.  Uses the
+ * default solve options with max_iter/tol overridden; verbose is ignored. */
+int cuphu_laplace_unwrap_gpu(const void *d_smooth_costs, const float *d_phase, int nrow,
+                             int ncol, double nshortcycle, int max_iter, float tol,
+                             int verbose, float *d_unw, void *stream);
+
+/* new: same with options, any cost element stride (2 = smooth, 4 = defo
+ * shorts per arc), an optional int32 cycle-map output k (unw = phi + 2 pi k)
+ * and an optional float output of the anchored continuous solution before
+ * the congruence projection */
+int cuphu_laplace_solve_device(const void *d_costs, int cost_stride_shorts,
+                               const float *d_phase, int nrow, int ncol,
+                               const CuPhuSolveOptions *opts, float *d_unw,
+                               int32_t *d_cycles, float *d_cont, CuPhuSolveStats *stats,
+                               void *stream);
+
+/* ── integration of MCF flows (ref cuphu.h:261-270, cuphu_phase.cu:110-144) */
+int cuphu_integrate_phase_gpu(const float *wrapped_phase, const short *hflows,
+                              const short *vflows, int nrow, int ncol, int gpu_id,
+                              float *unw_out);
+
+/* ── connected components (ref cuphu.h:275-289, cuphu_conncomp.cu:290-428) */
+int cuphu_conncomp_gpu(const float *unw, const float *corr, const unsigned char *mask,
+                       int nrow, int ncol, const short *poscost, const short *negcost,
+                       const CuPhuParams *params, int gpu_id, uint32_t *labels_out);
+
+/* new: host pointers, explicit coherence floor (regrow_conncomp semantics,
+ * ref _conncomp.py:12-66: valid = corr >= corr_thresh && mask) */
+int cuphu_conncomp_ex(const float *unw, const float *corr, const unsigned char *mask, int nrow,
+                      int ncol, float corr_thresh, double minfrac, long maxncomps, int gpu_id,
+                      uint32_t *labels_out);
+
+/* ── incremental costs (ref cuphu_incrcost.cu:157-191); returns 1 when no
+ *    negative incremental cost exists, 0 otherwise, negative on error */
+int cuphu_incrcost_early_exit(const void *d_costs_flat, const short *d_flows_flat,
+                              int narcs, long nshortcycle, int nflow, short *d_poscost,
+                              short *d_negcost, int *d_scratch);
+
+/* ── GPU queries (ref cuphu_py.cu:435-456) ─────────────────────────────── */
+int cuphu_gpu_count(void);
+int cuphu_gpu_name(int device, char *buf, int len);
+int cuphu_gpu_info(int device, long long *total_memory, int *sm_count, int *cc_major,
+                   int *cc_minor);
+
+/* wait for the last pipeline enqueued on a device and return its device-side
+ * status (CUPHU_ERR_TIMEOUT when a grid barrier gave up) (new) */
+int cuphu_last_status(int gpu_id);
+
+/* release the cached per-device workspace (new) */
+int cuphu_release_workspace(int gpu_id);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUPHU_B200_H */

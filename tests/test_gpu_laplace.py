@@ -1,0 +1,115 @@
+"""GPU Laplace solver parity.
+
+* FP64 mode against the CPU FP64 oracle: same operation order, explicit FMA
+  and the same reduction tree, so the cycle map, the congruent output and the
+  continuous solution agree bit for bit.
+* Mixed mode against FP64: continuous solutions within 1e-3 rad RMS and
+  cycle maps with at most a handful of mismatches (all at pixels whose
+  continuous solution sits within a hair of a half cycle).
+* The reference FP32 kernels (float-atomic dot products, nondeterministic)
+  are compared by cycle-map agreement fraction.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle as O
+from cuphu_b200 import synthetic as S
+from cuphu_b200._lib import CuPhuSolveStats, check, default_solve_options, lib
+from tests.devbuf import dptr, empty, to_dev, to_host
+
+pytestmark = pytest.mark.gpu
+
+
+def scene(nr, nc, seed, nlooks=5.0):
+    ig, g, t, _ = S.bumps(nr, nc, seed=seed, nbumps=3, amp_range=(10.0, 40.0),
+                          sigma_range=(10.0, 40.0), nlooks=nlooks)
+    ph = O.phase_from_igram(ig)
+    return ph, g, t
+
+
+def gpu_solve(torch, costs, ph, precision, n_irls=2, max_iter=1000, tol=1e-3):
+    nr, nc = ph.shape
+    dcost, dph = to_dev(costs), to_dev(ph)
+    du = empty((nr, nc), torch.float32)
+    dk = empty((nr, nc), torch.int32)
+    dcont = empty((nr, nc), torch.float32)
+    o = default_solve_options(precision=precision, n_irls=n_irls, max_iter=max_iter, tol=tol)
+    st = CuPhuSolveStats()
+    check(lib().cuphu_laplace_solve_device(dptr(dcost), costs.shape[1], dptr(dph), nr, nc,
+                                           C.byref(o), dptr(du), dptr(dk), dptr(dcont),
+                                           C.byref(st), None))
+    return to_host(du), to_host(dk), to_host(dcont), st
+
+
+@pytest.mark.parametrize("shape,seed,mode", [((64, 64), 1, 0), ((100, 130), 2, 1),
+                                             ((37, 211), 3, 0), ((160, 96), 4, 1)])
+def test_fp64_bit_exact_vs_oracle(torch_cuda, shape, seed, mode):
+    ph, g, _ = scene(*shape, seed)
+    costs = O.build_costs(ph, g, 5.0, mode=mode)
+    x, k, unw, iters = O.laplace_f64(costs, ph, O.lap_opts(n_irls=2))
+    gu, gk, gc, st = gpu_solve(torch_cuda, costs, ph, precision=1, n_irls=2)
+    assert st.total_iters == int(iters.sum())
+    assert np.array_equal(gk, k)
+    assert np.array_equal(gu.view(np.int32), unw.view(np.int32))
+    off = float(ph[0, 0]) - x[0, 0]
+    assert np.array_equal(gc, (x + off).astype(np.float32))
+
+
+def test_mixed_close_to_fp64(torch_cuda):
+    ph, g, _ = scene(256, 256, 7)
+    costs = O.build_costs(ph, g, 5.0, mode=1)
+    _, k64, c64, _ = gpu_solve(torch_cuda, costs, ph, precision=1, n_irls=4)
+    _, k32, c32, _ = gpu_solve(torch_cuda, costs, ph, precision=0, n_irls=4)
+    rms = float(np.sqrt(np.mean((c32.astype(np.float64) - c64) ** 2)))
+    mism = int(np.sum(k32 != k64))
+    assert rms < 1e-3, rms
+    assert mism <= max(3, int(1e-4 * k64.size)), mism
+
+
+def test_mixed_close_to_oracle_on_config_like_scene(torch_cuda):
+    ph, g, _ = scene(192, 160, 11, nlooks=9.0)
+    costs = O.build_costs(ph, g, 9.0, mode=0)
+    x, k, _, _ = O.laplace_f64(costs, ph, O.lap_opts(n_irls=3))
+    _, gk, gc, _ = gpu_solve(torch_cuda, costs, ph, precision=0, n_irls=3)
+    off = float(ph[0, 0]) - x[0, 0]
+    rms = float(np.sqrt(np.mean((gc.astype(np.float64) - (x + off)) ** 2)))
+    assert rms < 1e-3, rms
+    assert np.sum(gk != k) <= max(3, int(1e-4 * k.size))
+
+
+def test_solver_is_deterministic(torch_cuda):
+    ph, g, _ = scene(200, 240, 5)
+    costs = O.build_costs(ph, g, 5.0, mode=0)
+    for prec in (0, 1):
+        a = gpu_solve(torch_cuda, costs, ph, precision=prec, n_irls=2)
+        b = gpu_solve(torch_cuda, costs, ph, precision=prec, n_irls=2)
+        assert np.array_equal(a[2].view(np.int32), b[2].view(np.int32))
+
+
+def test_against_reference_fp32_kernels(torch_cuda):
+    if O.ref_lib() is None:
+        pytest.skip("reference kernels not built")
+    ph, g, _ = scene(128, 128, 9)
+    costs = O.build_costs(ph, g, 5.0, mode=0)
+    ref_unw, _ = O.ref_laplace(costs, ph)
+    gu, gk, _, _ = gpu_solve(torch_cuda, costs, ph, precision=0, n_irls=16)
+    kref = np.rint((ref_unw.astype(np.float64) - ph) / (2 * np.pi))
+    assert np.mean(kref != gk) < 0.02
+
+
+def test_max_iter_cap_and_zero_weights(torch_cuda):
+    ph, g, _ = scene(64, 80, 13)
+    costs = O.build_costs(ph, g, 5.0, mode=0)
+    _, _, _, st = gpu_solve(torch_cuda, costs, ph, precision=1, n_irls=1, max_iter=3)
+    assert st.max_iters_pass <= 3
+    x, k, unw, iters = O.laplace_f64(costs, ph, O.lap_opts(n_irls=1, max_iter=3))
+    gu, gk, _, _ = gpu_solve(torch_cuda, costs, ph, precision=1, n_irls=1, max_iter=3)
+    assert np.array_equal(gk, k)
+    masked = costs.copy()
+    masked[:, 1] = 32000                      # every arc masked: nothing to solve
+    gu, gk, _, st = gpu_solve(torch_cuda, masked, ph, precision=0, n_irls=1)
+    assert st.total_iters == 0
+    _, k0, u0, _ = O.laplace_f64(masked, ph, O.lap_opts(n_irls=1))
+    assert np.array_equal(gk, k0) and np.array_equal(gu, u0)
