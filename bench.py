@@ -196,6 +196,15 @@ def run_ours(args, rank, world, local_rank):
     if dist:
         import torch.distributed as tdist
     st = CuPhuSolveStats()
+    if args.profile:
+        # one warm-up and one device step, nothing else (for ncu captures)
+        for _ in range(args.warmup + 1):
+            step(opts, st)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_case": args.workload, "solve_ms": st.solve_ms,
+                          "total_ms": st.total_ms, "pcg_iterations": st.total_iters,
+                          "px_iterations": st.px_iters, "ntiles": st.ntiles}), flush=True)
+        return
     for _ in range(args.warmup):
         step(opts, st)
     torch.cuda.synchronize()
@@ -235,13 +244,14 @@ def run_ours(args, rank, world, local_rank):
     tr_f = [(int(t * (nrow - 64) / ntr), (nrow if t == ntr - 1 else int((t + 1) * (nrow - 64) / ntr) + 64)) for t in range(ntr)]
     tc_f = [(int(t * (ncol - 64) / ntc), (ncol if t == ntc - 1 else int((t + 1) * (ncol - 64) / ntc) + 64)) for t in range(ntc)]
     tile_px = sum((b - a) for a, b in tr_f) * sum((b - a) for a, b in tc_f)
-    px_iters = st.total_iters * tile_px  # upper bound: every tile active in every iteration
+    px_iters = st.px_iters                # iterations x pixels of the active tiles
     bpi = 36 if prec == 0 else 64
     alg_bytes = px_iters * bpi + (opts.n_irls + 1) * tile_px * 38
     achieved = alg_bytes / (st.solve_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
                 "kernel": "k_solve", "solve_ms": st.solve_ms, "pcg_iterations": st.total_iters,
+                "px_iterations": st.px_iters, "tile_px": tile_px,
                 "bytes_per_px_iter": bpi}
 
     result = {}
@@ -357,6 +367,8 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="warm-up + one device step only (for ncu captures)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

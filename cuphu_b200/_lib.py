@@ -78,7 +78,7 @@ class CuPhuSolveOptions(C.Structure):
 
 class CuPhuSolveStats(C.Structure):
     _fields_ = [("ntiles", _I), ("total_iters", _I), ("max_iters_pass", _I),
-                ("solve_ms", _D), ("total_ms", _D)]
+                ("solve_ms", _D), ("total_ms", _D), ("px_iters", _D)]
 
 
 class CuPhuScene(C.Structure):

@@ -146,7 +146,7 @@ struct Plan {
     std::vector<CostConsts> consts;
     std::vector<size_t> map_off;
     long long nplane = 0;
-    int nitems = 0, total_rows = 0;
+    int nitems = 0, total_rows = 0, pitch = 4;
 };
 
 static int plan_job(const std::vector<SceneIn> &S, const CuPhuParams &prm, Plan &pl)
@@ -192,9 +192,7 @@ static int plan_job(const std::vector<SceneIn> &S, const CuPhuParams &prm, Plan 
                 T.tr = tr;
                 T.tc = tc;
                 T.ph_pitch = in.ncol;
-                T.pitch = (T.nc + 3) & ~3;
-                T.pix = pl.nplane;
-                pl.nplane += (long long)T.nr * T.pitch;
+                T.pitch = (T.nc + 3) & ~3;   /* replaced by the common pitch below */
                 T.nbx = (T.nc + kItemBx - 1) / kItemBx;
                 int nby = (T.nr + kItemBy - 1) / kItemBy;
                 T.nitems = T.nbx * nby;
@@ -239,6 +237,15 @@ static int plan_job(const std::vector<SceneIn> &S, const CuPhuParams &prm, Plan 
         pl.maps.insert(pl.maps.end(), cm.begin(), cm.end());
         pl.scenes.push_back(sp);
     }
+    /* common pitch: tiles are stacked row-wise into one 2-D array per plane */
+    int P = 4;
+    for (auto &T : pl.tiles) P = std::max(P, T.pitch);
+    pl.pitch = P;
+    for (auto &T : pl.tiles) {
+        T.pitch = P;
+        T.pix = (long long)T.row0 * P;
+    }
+    pl.nplane = (long long)pl.total_rows * P;
     return 0;
 }
 
@@ -283,12 +290,13 @@ static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpt
         P.w0r = b.take<float>(np);
         P.wd = b.take<float>(np);
         P.wr = b.take<float>(np);
-        P.x = b.take<char>(np * vs);
+        P.x = b.take<double>(np);
         P.r = b.take<char>(np * vs);
         P.p0 = b.take<char>(np * vs);
         P.p1 = b.take<char>(np * vs);
         P.q = b.take<char>(np * vs);
         P.diag = b.take<char>(np * vs);
+        P.z = b.take<char>(np * vs);
         P.unw = b.take<float>(np);
         P.cyc = jo.want_cyc ? b.take<int32_t>(np) : nullptr;
         P.cont = jo.cont_out ? b.take<float>(np) : nullptr;
@@ -306,8 +314,8 @@ static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpt
         d_coff = b.take<unsigned>(ntiles);
         d_sout = b.take<SceneOut>(nsc);
         d_k = b.take<CostConsts>(nsc);
-        d_st = b.take<TileState>(ntiles);
-        d_part = b.take<double>(pl.nitems);
+        d_st = b.take<TileState>(2 * (size_t)ntiles);
+        d_part = b.take<double>(2 * (size_t)pl.nitems);
         d_ctl = b.take<SolverCtl>(1);
         d_deltas = b.take<float>(o.n_irls + 1);
         d_pass = b.take<int>(o.n_irls + 1);
@@ -388,7 +396,7 @@ static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpt
         deltas[k] = std::max(o.irls_delta_min, o.irls_delta_max * powf(0.5f, (float)k));
     CUPHU_TRY_CUDA(cudaMemcpyAsync(d_deltas, deltas.data(), deltas.size() * sizeof(float),
                                    cudaMemcpyHostToDevice, s));
-    CUPHU_TRY_CUDA(cudaMemsetAsync(d_st, 0, ntiles * sizeof(TileState), s));
+    CUPHU_TRY_CUDA(cudaMemsetAsync(d_st, 0, 2 * ntiles * sizeof(TileState), s));
     CUPHU_TRY_CUDA(cudaMemsetAsync(d_ctl, 0, sizeof(SolverCtl), s));
 
     for (int i = 0; i < nsc; ++i) {
@@ -414,8 +422,8 @@ static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpt
     sp.pass_iters = d_pass;
     sp.timeout_ns = (long long)std::max(1, o.timeout_ms) * 1000000LL;
     if (stats) cudaEventRecord(e1, s);
-    rc = launch_solve(jo.fp64, d_tiles, d_item, pl.nitems, ntiles, P, d_st, d_part, d_ctl, sp,
-                      dev, s);
+    rc = launch_solve(jo.fp64, d_tiles, d_item, pl.nitems, ntiles, P, pl.pitch, pl.total_rows, d_st,
+                      d_part, d_ctl, sp, dev, s);
     if (rc) return rc;
     if (stats) cudaEventRecord(e2, s);
     if (jo.want_cc) {
@@ -462,6 +470,7 @@ static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpt
         stats->max_iters_pass = ctl.max_pass_iters;
         stats->solve_ms = ms_solve;
         stats->total_ms = ms_total;
+        stats->px_iters = (double)ctl.px_iters;
         cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2); cudaEventDestroy(e3);
         if (ctl.err) return fail(CUPHU_ERR_TIMEOUT, "solver grid barrier timed out");
     }

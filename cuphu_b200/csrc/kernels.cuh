@@ -2,9 +2,10 @@
  * kernels.cuh -- device data structures shared by the kernels and the host
  * orchestrator, and the launcher declarations.
  *
- * HBM layout: every tile of every scene owns a slab of pitched planes
- * (pitch = ncol rounded up to 4 elements, so every row starts 16-byte
- * aligned for vector loads).  Arc weights live in two planes: wd[r][c] is
+ * HBM layout: the tiles of every scene of a job are stacked row-wise into
+ * one 2-D array per plane with a common pitch (the widest tile rounded up to
+ * 4 elements, so every row starts 16-byte aligned); one TMA tensor map per
+ * plane then addresses every tile.  Arc weights live in two planes: wd[r][c] is
  * the down arc (r,c)->(r+1,c) (the reference's row arc, cuphu_laplace.cu:85)
  * and wr[r][c] the right arc (r,c)->(r,c+1) (col arc, :86); the last row of
  * wd and the last column of wr are zero.  Scene-level arrays (phase, corr,
@@ -35,8 +36,10 @@ struct TileDesc {
 struct SolverPlanes {
     float *w0d, *w0r;           /* data weights 1/sigsq                  */
     float *wd, *wr;             /* current IRLS weights                  */
-    void *x, *r, *p0, *p1;      /* PCG state, float or double; p is     */
+    double *x;                  /* solution, FP64 in both precisions     */
+    void *r, *p0, *p1;          /* PCG vectors, float or double; p is    */
     void *q, *diag;             /* double-buffered across iterations     */
+    void *z;                    /* z = r / diag, written by the update pass */
     float *unw;                 /* congruent unwrapped phase per tile    */
     int32_t *cyc;               /* optional cycle map per tile           */
     float *cont;                /* optional anchored continuous solution */
@@ -44,16 +47,18 @@ struct SolverPlanes {
     uint32_t *aux;              /* component sizes, then root labels     */
 };
 
+/* per-tile PCG scalars, double-buffered by iteration parity: every block
+ * touching a tile derives the same values from the same partials */
 struct TileState {
     double rz, rz0, thr, alpha, beta;
-    int active, iter, pad0, pad1;
-    unsigned ticket, pad2;
+    int active, iter;
 };
 
 struct SolverCtl {
     unsigned bar_count, bar_gen;
     int err, n_active, snap;
     int total_iters, max_pass_iters, pad;
+    unsigned long long px_iters;   /* sum over tiles and passes of iterations x pixels */
 };
 
 struct SolveParams {
@@ -102,8 +107,9 @@ int launch_w0_from_costs(const short *costs, int stride, int nrow, int ncol, int
 
 /* laplace.cu */
 int launch_solve(bool fp64, const TileDesc *tiles, const int *item_tile, int nitems,
-                 int ntiles, const SolverPlanes &P, TileState *st, double *part,
-                 SolverCtl *ctl, const SolveParams &sp, int device, cudaStream_t s);
+                 int ntiles, const SolverPlanes &P, int plane_pitch, int plane_rows,
+                 TileState *st, double *part, SolverCtl *ctl, const SolveParams &sp,
+                 int device, cudaStream_t s);
 
 /* conncomp.cu */
 struct CcArgs {

@@ -27,6 +27,8 @@
  */
 #include "kernels.cuh"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda/atomic>
 #include <vector>
 
@@ -74,31 +76,26 @@ __device__ __forceinline__ double block_sum(double v, double *sw)
     return v;
 }
 
-/* Item partial -> per-tile ticket; the last block of the tile reduces the
- * tile's item partials in fixed order.  Returns true in the last block;
- * *total is valid in its thread 0. */
-__device__ __forceinline__ bool item_reduce(double acc, const TileDesc &T, int t, int item,
-                                            double *part, TileState *st, double *sw,
-                                            int *s_last, double *total)
+/* Tile total of the item partials of one phase, in fixed order: thread j
+ * sums items j, j+256, ... then the block tree.  Every block computes it the
+ * same way, so all blocks touching a tile agree bit for bit. */
+__device__ __forceinline__ double tile_reduce(const TileDesc &T, const double *part, double *sw,
+                                              double *s_bcast)
 {
-    double bs = block_sum(acc, sw);
-    if (threadIdx.x == 0) {
-        part[item] = bs;
-        __threadfence();
-        unsigned prev = atomicAdd(&st[t].ticket, 1u);
-        *s_last = (prev == (unsigned)T.nitems - 1u);
-    }
-    __syncthreads();
-    if (!*s_last) return false;
-    __threadfence();
     double a = 0.0;
     for (int i = threadIdx.x; i < T.nitems; i += blockDim.x) a = a + __ldcg(part + T.item0 + i);
     double tot = block_sum(a, sw);
-    if (threadIdx.x == 0) {
-        st[t].ticket = 0u;
-        *total = tot;
-    }
-    return true;
+    if (threadIdx.x == 0) *s_bcast = tot;
+    __syncthreads();
+    tot = *s_bcast;
+    __syncthreads();
+    return tot;
+}
+
+__device__ __forceinline__ void store_partial(double acc, double *part, int item, double *sw)
+{
+    double bs = block_sum(acc, sw);
+    if (threadIdx.x == 0) part[item] = bs;
 }
 
 __device__ __forceinline__ unsigned long long globaltimer()
@@ -167,7 +164,7 @@ __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, b
 {
     ItemXY q = item_xy(T, li);
     if (q.r >= T.nr || q.c0 >= T.nc) return 0.0;
-    V *x = (V *)P.x + T.pix;
+    double *x = P.x + T.pix;
     V *rr = (V *)P.r + T.pix;
     V *dg = (V *)P.diag + T.pix;
     const float *wd = P.wd + T.pix, *wr = P.wr + T.pix;
@@ -175,7 +172,8 @@ __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, b
     const double eps = (double)kLapEpsF;
     const int r = q.r, nr = T.nr, nc = T.nc, pitch = T.pitch, pp = T.ph_pitch;
     size_t prow = (size_t)r * pitch;
-    V xv[4], rv[4], dv[4];
+    double xv[4];
+    V rv[4], dv[4], zv[4];
     if (!zero_x) ld4(x + prow + q.c0, xv);
     if (!write_diag) ld4(dg + prow + q.c0, dv);
     double acc = 0.0;
@@ -184,8 +182,9 @@ __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, b
         int c = q.c0 + j;
         if (c >= nc) {
             rv[j] = (V)0;
+            zv[j] = (V)0;
             if (write_diag) dv[j] = (V)0;
-            if (zero_x) xv[j] = (V)0;
+            if (zero_x) xv[j] = 0.0;
             continue;
         }
         size_t gi = (size_t)r * pp + c, pi = prow + c;
@@ -227,140 +226,350 @@ __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, b
         double y;
         if (zero_x) {
             y = 0.0;
-            xv[j] = (V)0;
+            xv[j] = 0.0;
         } else {
-            double xa = (double)xv[j];
+            double xa = xv[j];
             y = eps * xa;
-            if (r < nr - 1) y = __fma_rn((double)ldc(wd + pi), xa - (double)ldc(x + pi + pitch), y);
-            if (r > 0)      y = __fma_rn((double)ldc(wd + pi - pitch), xa - (double)ldc(x + pi - pitch), y);
-            if (c < nc - 1) y = __fma_rn((double)ldc(wr + pi), xa - (double)ldc(x + pi + 1), y);
-            if (c > 0)      y = __fma_rn((double)ldc(wr + pi - 1), xa - (double)ldc(x + pi - 1), y);
+            if (r < nr - 1) y = __fma_rn((double)ldc(wd + pi), xa - ldc(x + pi + pitch), y);
+            if (r > 0)      y = __fma_rn((double)ldc(wd + pi - pitch), xa - ldc(x + pi - pitch), y);
+            if (c < nc - 1) y = __fma_rn((double)ldc(wr + pi), xa - ldc(x + pi + 1), y);
+            if (c > 0)      y = __fma_rn((double)ldc(wr + pi - 1), xa - ldc(x + pi - 1), y);
         }
         V rs = (V)(bv - y);
         V ds = (V)d;
         double z = (double)rs / (double)ds;
         acc = __fma_rn((double)rs, z, acc);
         rv[j] = rs;
+        zv[j] = (V)z;
         if (write_diag) dv[j] = ds;
     }
     st4(rr + prow + q.c0, rv);
+    st4((V *)P.z + T.pix + prow + q.c0, zv);
     if (write_diag) st4(dg + prow + q.c0, dv);
     if (zero_x) st4(x + prow + q.c0, xv);
     return acc;
 }
 
-/* ── stencil pass: p_new = z + beta p_old (own + halo, in shared memory),
- *    q = A p_new, partial p.q ─────────────────────────────────────────── */
-template <typename V>
-__device__ double phase_a(const TileDesc &T, int li, const SolverPlanes &P, const V *pold_all,
-                          V *pnew_all, bool first, double beta, V *smP)
+/* ── TMA-staged stencil and update passes ─────────────────────────────────
+ * Every plane of a job is one 2-D array (all tiles stacked row-wise with a
+ * common pitch), described by a TMA tensor map.  A block walks its work items
+ * through an NS-stage shared-memory ring: one thread issues the item's 2-D
+ * tensor copies (cp.async.bulk.tensor, no multicast) into a free stage and
+ * arms the stage's mbarrier with the box bytes; all threads compute on the
+ * oldest stage.  Boxes start at column c0b - 4 (16-byte aligned) and may
+ * reach outside the array; the TMA unit fills those elements with zeros and
+ * the kernels never read values outside the tile. */
+constexpr int kSegW = kItemBx + 8;        /* stencil box width: 4 columns each side */
+constexpr int kWrW = kItemBx + 4;         /* right-arc box incl. the left neighbour */
+
+struct SolveMaps {
+    CUtensorMap zA, p0A, p1A, wdA, wrA;        /* stencil pass boxes */
+    CUtensorMap xB, p0B, p1B, qB, rB, dB;      /* update pass boxes  */
+};
+
+__host__ __device__ constexpr size_t al128(size_t b) { return (b + 127) & ~(size_t)127; }
+
+template <typename V> struct StageA {
+    static constexpr size_t kVec = al128((size_t)(kItemBy + 2) * kSegW * sizeof(V));
+    static constexpr size_t kWd = al128((size_t)(kItemBy + 1) * kItemBx * sizeof(float));
+    static constexpr size_t kWr = al128((size_t)kItemBy * kWrW * sizeof(float));
+    static constexpr size_t kBytes = 2 * kVec + kWd + kWr;
+    static constexpr uint32_t kTx = (uint32_t)(2 * (kItemBy + 2) * kSegW * sizeof(V) +
+                                               (kItemBy + 1) * kItemBx * 4 + kItemBy * kWrW * 4);
+};
+template <typename V> struct StageB {
+    static constexpr size_t kX = (size_t)kItemBy * kItemBx * sizeof(double);
+    static constexpr size_t kV = (size_t)kItemBy * kItemBx * sizeof(V);
+    static constexpr size_t kBytes = kX + 4 * kV;
+    static constexpr uint32_t kTxFull = (uint32_t)(kX + 4 * kV);
+    static constexpr uint32_t kTxX = (uint32_t)(kX + kV);
+};
+template <typename V> __host__ __device__ constexpr int n_stages() { return sizeof(V) == 4 ? 3 : 2; }
+template <typename V> __host__ __device__ constexpr size_t stage_bytes()
 {
-    ItemXY q = item_xy(T, li);
-    const V *rr = (const V *)P.r + T.pix;
-    const V *dg = (const V *)P.diag + T.pix;
-    const V *po = pold_all + T.pix;
-    V *pn_out = pnew_all + T.pix;
-    V *qo = (V *)P.q + T.pix;
-    const float *wd = P.wd + T.pix, *wr = P.wr + T.pix;
-    const int nr = T.nr, nc = T.nc, pitch = T.pitch, r = q.r;
-    const bool own = r < nr && q.c0 < nc;
-    size_t prow = (size_t)r * pitch;
-    V pn[4] = {(V)0, (V)0, (V)0, (V)0};
-    if (own) {
-        V rv[4], dv[4], pv[4];
-        ld4(rr + prow + q.c0, rv);
-        ld4(dg + prow + q.c0, dv);
-        if (!first) ld4(po + prow + q.c0, pv);
-#pragma unroll
-        for (int j = 0; j < kItemVx; ++j) {
-            if (q.c0 + j >= nc) continue;
-            double z = (double)rv[j] / (double)dv[j];
-            pn[j] = (V)(first ? z : __fma_rn(beta, (double)pv[j], z));
+    return al128(StageA<V>::kBytes > StageB<V>::kBytes ? StageA<V>::kBytes : StageB<V>::kBytes);
+}
+template <typename V> __host__ __device__ constexpr size_t pn_bytes()
+{
+    return al128((size_t)kHaloH * kHaloW * sizeof(V));
+}
+template <typename V> __host__ __device__ constexpr size_t solve_smem_bytes()
+{
+    return n_stages<V>() * stage_bytes<V>() + pn_bytes<V>() + 128;
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y,
+                                            uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_addr(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(smem_addr(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+/* bounded wait for a stage; on timeout the error status is raised and the
+ * next grid barrier ends the kernel */
+__device__ __forceinline__ void mbar_wait(uint64_t *bar, uint32_t parity, SolverCtl *ctl,
+                                          long long timeout_ns)
+{
+    if (mbar_try(bar, parity)) return;
+    unsigned long long t0 = globaltimer();
+    for (long long i = 1;; ++i) {
+        if (mbar_try(bar, parity)) return;
+        if ((i & 255) == 0) {
+            if ((long long)(globaltimer() - t0) > timeout_ns || i > (1LL << 30)) {
+                atomicExch(&ctl->err, 2);
+                return;
+            }
         }
     }
-    const int srow = (q.ty + 1) * kHaloW + q.tx * kItemVx + 1;
-#pragma unroll
-    for (int j = 0; j < kItemVx; ++j) smP[srow + j] = pn[j];
-    /* halo ring (no corners: 5-point stencil) */
-    const int rb = (li / T.nbx) * kItemBy, cb = (li % T.nbx) * kItemBx;
-    for (int h = threadIdx.x; h < 2 * kItemBx + 2 * kItemBy; h += blockDim.x) {
-        int hr, hc, sidx;
-        if (h < kItemBx) { hr = rb - 1; hc = cb + h; sidx = h + 1; }
-        else if (h < 2 * kItemBx) { hr = rb + kItemBy; hc = cb + h - kItemBx; sidx = (kItemBy + 1) * kHaloW + h - kItemBx + 1; }
-        else if (h < 2 * kItemBx + kItemBy) { hr = rb + h - 2 * kItemBx; hc = cb - 1; sidx = (hr - rb + 1) * kHaloW; }
-        else { hr = rb + h - 2 * kItemBx - kItemBy; hc = cb + kItemBx; sidx = (hr - rb + 1) * kHaloW + kItemBx + 1; }
+}
+__device__ __forceinline__ void fence_async_smem()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_global()
+{
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
+template <typename V>
+__device__ __forceinline__ void issue_a(const TileDesc &T, int li, const SolveMaps &M, int pold_sel,
+                                        bool first, char *stage, uint64_t *bar)
+{
+    const int r0b = (li / T.nbx) * kItemBy, c0b = (li % T.nbx) * kItemBx;
+    const int y = T.row0 + r0b;
+    char *Z = stage;
+    char *PO = stage + StageA<V>::kVec;
+    char *WD = PO + StageA<V>::kVec;
+    char *WR = WD + StageA<V>::kWd;
+    uint32_t tx = StageA<V>::kTx - (first ? (uint32_t)((kItemBy + 2) * kSegW * sizeof(V)) : 0u);
+    mbar_expect(bar, tx);
+    tma_load_2d(Z, &M.zA, c0b - 4, y - 1, bar);
+    if (!first) tma_load_2d(PO, pold_sel ? &M.p1A : &M.p0A, c0b - 4, y - 1, bar);
+    tma_load_2d(WD, &M.wdA, c0b, y - 1, bar);
+    tma_load_2d(WR, &M.wrA, c0b - 4, y, bar);
+}
+
+/* stencil pass on a staged item: p_new = z + beta p_old (own + halo ring),
+ * q = A p_new, partial p.q */
+template <typename V>
+__device__ double compute_a(const TileDesc &T, int li, const SolverPlanes &P, V *pnew_all,
+                            bool first, double beta, const char *stage, V *Pn)
+{
+    const int r0b = (li / T.nbx) * kItemBy, c0b = (li % T.nbx) * kItemBx;
+    const V *Z = (const V *)stage;
+    const V *PO = (const V *)(stage + StageA<V>::kVec);
+    const float *WD = (const float *)(stage + 2 * StageA<V>::kVec);
+    const float *WR = (const float *)(stage + 2 * StageA<V>::kVec + StageA<V>::kWd);
+    const int nr = T.nr, nc = T.nc;
+    for (int k = threadIdx.x; k < kHaloH * kHaloW; k += blockDim.x) {
+        int i = k / kHaloW, j = k % kHaloW;
+        int gr = r0b - 1 + i, gc = c0b - 1 + j;
         V v = (V)0;
-        if (hr >= 0 && hr < nr && hc >= 0 && hc < nc) {
-            size_t pi = (size_t)hr * pitch + hc;
-            double z = (double)ldc(rr + pi) / (double)ldc(dg + pi);
-            v = (V)(first ? z : __fma_rn(beta, (double)ldc(po + pi), z));
+        if (gr >= 0 && gr < nr && gc >= 0 && gc < nc) {
+            int sidx = i * kSegW + j + 3;
+            double z = (double)Z[sidx];
+            v = (V)(first ? z : __fma_rn(beta, (double)PO[sidx], z));
         }
-        smP[sidx] = v;
+        Pn[k] = v;
     }
     __syncthreads();
+    const int ty = threadIdx.x / kItemTx, tx = threadIdx.x % kItemTx;
+    const int r = r0b + ty, c0 = c0b + tx * kItemVx;
     double acc = 0.0;
-    if (own) {
-        float wdn[4], wup[4] = {0.f, 0.f, 0.f, 0.f}, wrt[4];
-        ld4(wd + prow + q.c0, wdn);
-        if (r > 0) ld4(wd + prow - pitch + q.c0, wup);
-        ld4(wr + prow + q.c0, wrt);
-        float wlf = q.c0 > 0 ? ldc(wr + prow + q.c0 - 1) : 0.0f;
-        V qv[4] = {(V)0, (V)0, (V)0, (V)0};
+    if (r < nr && c0 < nc) {
+        V pn[4] = {(V)0, (V)0, (V)0, (V)0}, qv[4] = {(V)0, (V)0, (V)0, (V)0};
         const double eps = (double)kLapEpsF;
 #pragma unroll
         for (int j = 0; j < kItemVx; ++j) {
-            int c = q.c0 + j;
+            int c = c0 + j;
             if (c >= nc) continue;
-            int s = srow + j;
+            int s = (ty + 1) * kHaloW + tx * kItemVx + j + 1;
+            pn[j] = Pn[s];
             double xa = (double)pn[j];
             double y = eps * xa;
-            if (r < nr - 1) y = __fma_rn((double)wdn[j], xa - (double)smP[s + kHaloW], y);
-            if (r > 0)      y = __fma_rn((double)wup[j], xa - (double)smP[s - kHaloW], y);
-            if (c < nc - 1) y = __fma_rn((double)wrt[j], xa - (double)smP[s + 1], y);
-            if (c > 0)      y = __fma_rn((double)(j == 0 ? wlf : wrt[j - 1]), xa - (double)smP[s - 1], y);
+            int wc = tx * kItemVx + j;
+            if (r < nr - 1) y = __fma_rn((double)WD[(ty + 1) * kItemBx + wc], xa - (double)Pn[s + kHaloW], y);
+            if (r > 0)      y = __fma_rn((double)WD[ty * kItemBx + wc], xa - (double)Pn[s - kHaloW], y);
+            if (c < nc - 1) y = __fma_rn((double)WR[ty * kWrW + wc + 4], xa - (double)Pn[s + 1], y);
+            if (c > 0)      y = __fma_rn((double)WR[ty * kWrW + wc + 3], xa - (double)Pn[s - 1], y);
             qv[j] = (V)y;
             acc = __fma_rn((double)pn[j], (double)qv[j], acc);
         }
-        st4(pn_out + prow + q.c0, pn);
-        st4(qo + prow + q.c0, qv);
+        size_t o = T.pix + (size_t)r * T.pitch + c0;
+        st4(pnew_all + o, pn);
+        st4((V *)P.q + o, qv);
     }
-    __syncthreads();
     return acc;
 }
 
-/* ── update pass: x += alpha p, r -= alpha q, z = r/diag, partial r.z ──── */
 template <typename V>
-__device__ double phase_b(const TileDesc &T, int li, const SolverPlanes &P, const V *pnew_all,
-                          double alpha, bool update_r)
+__device__ __forceinline__ void issue_b(const TileDesc &T, int li, const SolveMaps &M, int pnew_sel,
+                                        bool update_r, char *stage, uint64_t *bar)
 {
-    ItemXY q = item_xy(T, li);
-    if (q.r >= T.nr || q.c0 >= T.nc) return 0.0;
-    size_t o = T.pix + (size_t)q.r * T.pitch + q.c0;
-    V *x = (V *)P.x + o;
-    V *rr = (V *)P.r + o;
-    V xv[4], pv[4], qv[4], rv[4], dv[4];
-    ld4(x, xv);
-    ld4(pnew_all + o, pv);
+    const int r0b = (li / T.nbx) * kItemBy, c0b = (li % T.nbx) * kItemBx;
+    const int y = T.row0 + r0b;
+    char *X = stage;
+    char *PB = X + StageB<V>::kX;
+    char *QB = PB + StageB<V>::kV;
+    char *RB = QB + StageB<V>::kV;
+    char *DB = RB + StageB<V>::kV;
+    mbar_expect(bar, update_r ? StageB<V>::kTxFull : StageB<V>::kTxX);
+    tma_load_2d(X, &M.xB, c0b, y, bar);
+    tma_load_2d(PB, pnew_sel ? &M.p1B : &M.p0B, c0b, y, bar);
     if (update_r) {
-        ld4((const V *)P.q + o, qv);
-        ld4(rr, rv);
-        ld4((const V *)P.diag + o, dv);
+        tma_load_2d(QB, &M.qB, c0b, y, bar);
+        tma_load_2d(RB, &M.rB, c0b, y, bar);
+        tma_load_2d(DB, &M.dB, c0b, y, bar);
     }
+}
+
+template <typename V>
+__device__ double compute_b(const TileDesc &T, int li, const SolverPlanes &P, double alpha,
+                            bool update_r, const char *stage)
+{
+    const int r0b = (li / T.nbx) * kItemBy, c0b = (li % T.nbx) * kItemBx;
+    const double *X = (const double *)stage;
+    const V *PB = (const V *)(stage + StageB<V>::kX);
+    const V *QB = PB + kItemBy * kItemBx;
+    const V *RB = QB + kItemBy * kItemBx;
+    const V *DB = RB + kItemBy * kItemBx;
+    const int ty = threadIdx.x / kItemTx, tx = threadIdx.x % kItemTx;
+    const int r = r0b + ty, c0 = c0b + tx * kItemVx;
+    if (r >= T.nr || c0 >= T.nc) return 0.0;
+    const int s0 = ty * kItemBx + tx * kItemVx;
+    double xv[4];
+    V rv[4], zv[4];
     double acc = 0.0;
 #pragma unroll
     for (int j = 0; j < kItemVx; ++j) {
-        if (q.c0 + j >= T.nc) continue;
-        xv[j] = (V)__fma_rn(alpha, (double)pv[j], (double)xv[j]);
+        xv[j] = X[s0 + j];
+        rv[j] = update_r ? RB[s0 + j] : (V)0;
+        zv[j] = (V)0;
+        if (c0 + j >= T.nc) continue;
+        xv[j] = __fma_rn(alpha, (double)PB[s0 + j], xv[j]);
         if (update_r) {
-            V rn = (V)__fma_rn(-alpha, (double)qv[j], (double)rv[j]);
+            V rn = (V)__fma_rn(-alpha, (double)QB[s0 + j], (double)rv[j]);
             rv[j] = rn;
-            double z = (double)rn / (double)dv[j];
+            double z = (double)rn / (double)DB[s0 + j];
+            zv[j] = (V)z;
             acc = __fma_rn((double)rn, z, acc);
         }
     }
-    st4(x, xv);
-    if (update_r) st4(rr, rv);
+    size_t o = T.pix + (size_t)r * T.pitch + c0;
+    st4(P.x + o, xv);
+    if (update_r) {
+        st4((V *)P.r + o, rv);
+        st4((V *)P.z + o, zv);
+    }
     return acc;
+}
+
+__device__ __forceinline__ int next_active_item(int item, int i1, const int *item_tile,
+                                                const TileDesc *tiles, const TileState *st)
+{
+    while (item < i1) {
+        int t = item_tile[item];
+        if (__ldcg(&st[t].active)) return item;
+        item = tiles[t].item0 + tiles[t].nitems;
+    }
+    return i1;
+}
+
+/* NS-stage ring of a block */
+struct Pipe {
+    char *stage[4];
+    uint64_t *bar;
+    uint32_t uses[4];
+    int ns;
+};
+
+/* run a staged pass over this block's items of active tiles.  KIND 0: the
+ * stencil pass, KIND 1: the update pass */
+template <int KIND, typename V>
+__device__ void run_pass(const TileDesc *tiles, const int *item_tile, int i0, int i1,
+                         const SolverPlanes &P, const SolveMaps &M, const TileState *st,
+                         int psel, V *pvec, bool flag, double *part, double *sw, V *Pn, Pipe &pp,
+                         SolverCtl *ctl, long long timeout_ns)
+{
+    int q[4];   /* items in flight, oldest first */
+    int nq = 0;
+    int nxt = next_active_item(i0, i1, item_tile, tiles, st);
+    if (nxt >= i1) return;
+    if (threadIdx.x == 0) {
+        fence_async_global();
+        fence_async_smem();
+    }
+    int issued = 0, done = 0;
+    /* prologue: fill ns - 1 stages */
+    while (nq < pp.ns - 1 && nxt < i1) {
+        if (threadIdx.x == 0) {
+            const TileDesc &T = tiles[item_tile[nxt]];
+            int sidx = issued % pp.ns;
+            if (KIND == 0) issue_a<V>(T, nxt - T.item0, M, psel, flag, pp.stage[sidx], &pp.bar[sidx]);
+            else issue_b<V>(T, nxt - T.item0, M, psel, flag, pp.stage[sidx], &pp.bar[sidx]);
+        }
+        q[nq++] = nxt;
+        ++issued;
+        nxt = next_active_item(nxt + 1, i1, item_tile, tiles, st);
+    }
+    while (nq > 0) {
+        if (nxt < i1) {
+            if (threadIdx.x == 0) {
+                fence_async_smem();
+                const TileDesc &T = tiles[item_tile[nxt]];
+                int sidx = issued % pp.ns;
+                if (KIND == 0) issue_a<V>(T, nxt - T.item0, M, psel, flag, pp.stage[sidx], &pp.bar[sidx]);
+                else issue_b<V>(T, nxt - T.item0, M, psel, flag, pp.stage[sidx], &pp.bar[sidx]);
+            }
+            q[nq++] = nxt;
+            ++issued;
+            nxt = next_active_item(nxt + 1, i1, item_tile, tiles, st);
+        }
+        int cur = q[0];
+        for (int k = 1; k < nq; ++k) q[k - 1] = q[k];
+        --nq;
+        int sidx = done % pp.ns;
+        mbar_wait(&pp.bar[sidx], pp.uses[sidx] & 1u, ctl, timeout_ns);
+        pp.uses[sidx]++;
+        ++done;
+        int t = item_tile[cur];
+        const TileDesc &T = tiles[t];
+        double acc;
+        if (KIND == 0) {
+            acc = compute_a<V>(T, cur - T.item0, P, pvec, flag, __ldcg(&st[t].beta), pp.stage[sidx], Pn);
+            store_partial(acc, part, cur, sw);
+        } else {
+            acc = compute_b<V>(T, cur - T.item0, P, __ldcg(&st[t].alpha), flag, pp.stage[sidx]);
+            if (flag) store_partial(acc, part, cur, sw);
+        }
+        __syncthreads();
+    }
 }
 
 /* ── IRLS reweight (A13): w = w0 / sqrt(e^2 + delta^2) ───────────────────── */
@@ -369,7 +578,7 @@ __device__ void phase_rw(const TileDesc &T, int li, const SolverPlanes &P, float
 {
     ItemXY q = item_xy(T, li);
     if (q.r >= T.nr || q.c0 >= T.nc) return;
-    const V *x = (const V *)P.x + T.pix;
+    const double *x = P.x + T.pix;
     const double dd = (double)delta * (double)delta;
     const int r = q.r, nr = T.nr, nc = T.nc, pitch = T.pitch, pp = T.ph_pitch;
     size_t prow = (size_t)r * pitch;
@@ -380,13 +589,13 @@ __device__ void phase_rw(const TileDesc &T, int li, const SolverPlanes &P, float
         wdo[j] = 0.0f; wro[j] = 0.0f;
         if (c >= nc) continue;
         size_t pi = prow + c, gi = (size_t)r * pp + c;
-        double xa = (double)ldc(x + pi);
+        double xa = ldc(x + pi);
         float pa = __ldg(T.ph + gi);
         if (r < nr - 1) {
             float w0 = __ldg(P.w0d + T.pix + pi);
             if (w0 > 0.0f) {
                 float g = lap_wrap_pi(__ldg(T.ph + gi + pp) - pa);
-                double e = ((double)ldc(x + pi + pitch) - xa) - (double)g;
+                double e = (ldc(x + pi + pitch) - xa) - (double)g;
                 wdo[j] = (float)((double)w0 / __dsqrt_rn(__fma_rn(e, e, dd)));
             }
         }
@@ -394,7 +603,7 @@ __device__ void phase_rw(const TileDesc &T, int li, const SolverPlanes &P, float
             float w0 = __ldg(P.w0r + T.pix + pi);
             if (w0 > 0.0f) {
                 float g = lap_wrap_pi(__ldg(T.ph + gi + 1) - pa);
-                double e = ((double)ldc(x + pi + 1) - xa) - (double)g;
+                double e = (ldc(x + pi + 1) - xa) - (double)g;
                 wro[j] = (float)((double)w0 / __dsqrt_rn(__fma_rn(e, e, dd)));
             }
         }
@@ -409,8 +618,8 @@ __device__ void phase_final(const TileDesc &T, int li, const SolverPlanes &P)
 {
     ItemXY q = item_xy(T, li);
     if (q.r >= T.nr || q.c0 >= T.nc) return;
-    const V *x = (const V *)P.x + T.pix;
-    double off = (double)__ldg(T.ph) - (double)ldc(x);
+    const double *x = P.x + T.pix;
+    double off = (double)__ldg(T.ph) - ldc(x);
     size_t prow = (size_t)q.r * T.pitch;
     float uo[4] = {0.f, 0.f, 0.f, 0.f}, co[4] = {0.f, 0.f, 0.f, 0.f};
     int ko[4] = {0, 0, 0, 0};
@@ -419,7 +628,7 @@ __device__ void phase_final(const TileDesc &T, int li, const SolverPlanes &P)
         int c = q.c0 + j;
         if (c >= T.nc) continue;
         float ph = __ldg(T.ph + (size_t)q.r * T.ph_pitch + c);
-        double u = (double)ldc(x + prow + c) + off;
+        double u = ldc(x + prow + c) + off;
         double d = u - (double)ph;
         double k = rint(d / kTwoPiD);
         co[j] = (float)u;
@@ -433,95 +642,167 @@ __device__ void phase_final(const TileDesc &T, int li, const SolverPlanes &P)
         *reinterpret_cast<float4 *>(P.cont + T.pix + prow + q.c0) = make_float4(co[0], co[1], co[2], co[3]);
 }
 
-__device__ __forceinline__ void finish_iter(TileState &S, double rzn, int max_iter, SolverCtl *ctl)
+/* Block b owns the contiguous work-item range [b*n/G, (b+1)*n/G); items are
+ * tile-major, so a block touches one or a few consecutive tiles.  The owner
+ * of a tile (the block holding its first item) maintains the global count of
+ * active tiles. */
+struct Range {
+    int i0, i1, t0, t1;
+};
+
+/* state written by other blocks before the last grid barrier: read from L2 */
+__device__ __forceinline__ TileState load_state(const TileState *p)
 {
-    S.iter += 1;
-    if (rzn < S.thr || S.iter >= max_iter) {
-        S.active = 0;
-        atomicSub(&ctl->n_active, 1);
-    } else {
-        S.beta = rzn / S.rz;
-        S.rz = rzn;
-    }
+    TileState S;
+    S.rz = __ldcg(&p->rz);
+    S.rz0 = __ldcg(&p->rz0);
+    S.thr = __ldcg(&p->thr);
+    S.alpha = __ldcg(&p->alpha);
+    S.beta = __ldcg(&p->beta);
+    S.active = __ldcg(&p->active);
+    S.iter = __ldcg(&p->iter);
+    return S;
 }
 
-template <typename V>
-__global__ void __launch_bounds__(kItemThreads) k_solve(const TileDesc *__restrict__ tiles,
-                                                        const int *__restrict__ item_tile,
-                                                        int nitems, SolverPlanes P,
-                                                        TileState *st, double *part,
-                                                        SolverCtl *ctl, SolveParams sp,
-                                                        long long timeout_ns)
+__device__ __forceinline__ Range block_range(const int *item_tile, int nitems)
 {
-    __shared__ V smP[kHaloH * kHaloW];
+    Range R;
+    R.i0 = (int)((long long)blockIdx.x * nitems / gridDim.x);
+    R.i1 = (int)((long long)(blockIdx.x + 1) * nitems / gridDim.x);
+    R.t0 = R.i0 < R.i1 ? item_tile[R.i0] : 0;
+    R.t1 = R.i0 < R.i1 ? item_tile[R.i1 - 1] : -1;
+    return R;
+}
+
+#ifndef CUPHU_SOLVE_MIN_BLOCKS
+#define CUPHU_SOLVE_MIN_BLOCKS 2
+#endif
+
+template <typename V>
+__global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
+    k_solve(const TileDesc *__restrict__ tiles, const int *__restrict__ item_tile, int nitems,
+            int ntiles, SolverPlanes P, TileState *st, double *part, SolverCtl *ctl,
+            SolveParams sp, long long timeout_ns, const __grid_constant__ SolveMaps M)
+{
+    extern __shared__ __align__(128) char dsm_raw[];
     __shared__ double sw[32];
-    __shared__ int s_last;
+    __shared__ double s_bcast;
+    __shared__ __align__(8) uint64_t bars[4];
+    char *dsm = (char *)(((uintptr_t)dsm_raw + 127) & ~(uintptr_t)127);
     const bool mixed = sizeof(V) == 4;
     V *pb[2] = {(V *)P.p0, (V *)P.p1};
-    double tot = 0.0;
+    double *pbuf[2] = {part, part + nitems};
+    const Range R = block_range(item_tile, nitems);
+    Pipe pp;
+    pp.ns = n_stages<V>();
+    for (int k = 0; k < pp.ns; ++k) {
+        pp.stage[k] = dsm + k * stage_bytes<V>();
+        pp.uses[k] = 0u;
+    }
+    pp.bar = bars;
+    V *Pn = (V *)(dsm + pp.ns * stage_bytes<V>());
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < pp.ns; ++k) mbar_init(&bars[k]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    int pc = 0;   /* phase counter selecting the partial buffer */
 
     for (int outer = 0; outer <= sp.n_irls; ++outer) {
-        /* assemble b, diag; r = b - A x; rz0 */
-        for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
-            int t = item_tile[item];
+        /* assemble b, diag; r = b - A x; partial r.z */
+        for (int t = R.t0; t <= R.t1; ++t) {
             const TileDesc &T = tiles[t];
-            double acc = phase_init<V>(T, item - T.item0, P, outer == 0, true);
-            if (item_reduce(acc, T, t, item, part, st, sw, &s_last, &tot) && threadIdx.x == 0) {
-                TileState &S = st[t];
-                S.rz = tot;
-                S.rz0 = tot;
-                S.thr = (double)sp.tol * (double)sp.tol * tot;
-                S.iter = 0;
-                S.beta = 0.0;
-                S.active = tot > 0.0 ? 1 : 0;
-                if (S.active) atomicAdd(&ctl->n_active, 1);
-            }
+            int a = max(R.i0, T.item0), b = min(R.i1, T.item0 + T.nitems);
+            for (int item = a; item < b; ++item)
+                store_partial(phase_init<V>(T, item - T.item0, P, outer == 0, true),
+                              pbuf[pc & 1], item, sw);
         }
+        ++pc;
         if (!grid_sync(ctl, timeout_ns)) return;
 
         int it = 0;
-        while (*(volatile int *)&ctl->snap > 0 && it < sp.max_iter) {
-            const V *pold = pb[it & 1];
+        while (true) {
+            TileState *cur = st + (it & 1) * ntiles;
+            TileState *nxt = st + ((it + 1) & 1) * ntiles;
             V *pnew = pb[(it + 1) & 1];
-            for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
-                int t = item_tile[item];
-                if (!*(volatile int *)&st[t].active) continue;
+            /* reduce r.z of the previous phase and update the tile scalars */
+            for (int t = R.t0; t <= R.t1; ++t) {
                 const TileDesc &T = tiles[t];
-                double beta = *(volatile double *)&st[t].beta;
-                double acc = phase_a<V>(T, item - T.item0, P, pold, pnew, it == 0, beta, smP);
-                if (item_reduce(acc, T, t, item, part, st, sw, &s_last, &tot) && threadIdx.x == 0) {
-                    TileState &S = st[t];
-                    if (tot <= 0.0) {
-                        S.active = 0;
-                        atomicSub(&ctl->n_active, 1);
-                    } else {
-                        S.alpha = S.rz / tot;
+                const bool owner = T.item0 >= R.i0 && T.item0 < R.i1;
+                TileState S;
+                if (it == 0) {
+                    double tot = tile_reduce(T, pbuf[(pc - 1) & 1], sw, &s_bcast);
+                    S.rz = tot;
+                    S.rz0 = tot;
+                    S.thr = (double)sp.tol * (double)sp.tol * tot;
+                    S.alpha = 0.0;
+                    S.beta = 0.0;
+                    S.iter = 0;
+                    S.active = (tot > 0.0 && sp.max_iter > 0) ? 1 : 0;
+                    if (owner && threadIdx.x == 0 && S.active) atomicAdd(&ctl->n_active, 1);
+                } else {
+                    S = load_state(cur + t);
+                    if (S.active) {
+                        double tot = tile_reduce(T, pbuf[(pc - 1) & 1], sw, &s_bcast);
+                        S.iter += 1;
+                        if (tot < S.thr || S.iter >= sp.max_iter) {
+                            S.active = 0;
+                            if (owner && threadIdx.x == 0) {
+                                atomicSub(&ctl->n_active, 1);
+                                atomicAdd(&ctl->px_iters, (unsigned long long)S.iter *
+                                                              (unsigned long long)((long long)T.nr * T.nc));
+                            }
+                        } else {
+                            S.beta = tot / S.rz;
+                            S.rz = tot;
+                        }
                     }
                 }
+                if (threadIdx.x == 0) nxt[t] = S;
             }
+            __syncthreads();
+            /* stencil pass */
+            run_pass<0, V>(tiles, item_tile, R.i0, R.i1, P, M, nxt, it & 1, pnew, it == 0,
+                           pbuf[pc & 1], sw, Pn, pp, ctl, timeout_ns);
+            ++pc;
             if (!grid_sync(ctl, timeout_ns)) return;
+            if (*(volatile int *)&ctl->snap <= 0) break;
+
+            /* reduce p.q, alpha (pq <= 0 ends the tile's solve) */
             const bool repl = mixed && sp.replace_every > 0 && ((it + 1) % sp.replace_every) == 0;
-            for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
-                int t = item_tile[item];
-                if (!*(volatile int *)&st[t].active) continue;
+            for (int t = R.t0; t <= R.t1; ++t) {
                 const TileDesc &T = tiles[t];
-                double alpha = *(volatile double *)&st[t].alpha;
-                double acc = phase_b<V>(T, item - T.item0, P, pnew, alpha, !repl);
-                if (!repl && item_reduce(acc, T, t, item, part, st, sw, &s_last, &tot) &&
-                    threadIdx.x == 0)
-                    finish_iter(st[t], tot, sp.max_iter, ctl);
+                const bool owner = T.item0 >= R.i0 && T.item0 < R.i1;
+                TileState S = load_state(nxt + t);
+                if (!S.active) continue;
+                double pq = tile_reduce(T, pbuf[(pc - 1) & 1], sw, &s_bcast);
+                if (pq <= 0.0) {
+                    if (threadIdx.x == 0) nxt[t].active = 0;
+                    if (owner && threadIdx.x == 0) {
+                        atomicSub(&ctl->n_active, 1);
+                        atomicAdd(&ctl->px_iters, (unsigned long long)S.iter *
+                                                      (unsigned long long)((long long)T.nr * T.nc));
+                    }
+                } else if (threadIdx.x == 0) {
+                    nxt[t].alpha = S.rz / pq;
+                }
             }
+            __syncthreads();
+            /* update pass (with periodic true residual in mixed precision) */
+            run_pass<1, V>(tiles, item_tile, R.i0, R.i1, P, M, nxt, (it + 1) & 1, pnew, !repl,
+                           pbuf[pc & 1], sw, Pn, pp, ctl, timeout_ns);
+            if (!repl) ++pc;
             if (!grid_sync(ctl, timeout_ns)) return;
             if (repl) {
-                for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
-                    int t = item_tile[item];
-                    if (!*(volatile int *)&st[t].active) continue;
+                for (int t = R.t0; t <= R.t1; ++t) {
                     const TileDesc &T = tiles[t];
-                    double acc = phase_init<V>(T, item - T.item0, P, false, false);
-                    if (item_reduce(acc, T, t, item, part, st, sw, &s_last, &tot) &&
-                        threadIdx.x == 0)
-                        finish_iter(st[t], tot, sp.max_iter, ctl);
+                    if (!__ldcg(&nxt[t].active)) continue;
+                    int a = max(R.i0, T.item0), b = min(R.i1, T.item0 + T.nitems);
+                    for (int item = a; item < b; ++item)
+                        store_partial(phase_init<V>(T, item - T.item0, P, false, false),
+                                      pbuf[pc & 1], item, sw);
                 }
+                ++pc;
                 if (!grid_sync(ctl, timeout_ns)) return;
             }
             ++it;
@@ -533,59 +814,119 @@ __global__ void __launch_bounds__(kItemThreads) k_solve(const TileDesc *__restri
         }
         if (outer < sp.n_irls) {
             float delta = sp.deltas[outer];
-            for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
-                int t = item_tile[item];
+            for (int t = R.t0; t <= R.t1; ++t) {
                 const TileDesc &T = tiles[t];
-                phase_rw<V>(T, item - T.item0, P, delta);
+                int a = max(R.i0, T.item0), b = min(R.i1, T.item0 + T.nitems);
+                for (int item = a; item < b; ++item) phase_rw<V>(T, item - T.item0, P, delta);
             }
             if (!grid_sync(ctl, timeout_ns)) return;
         }
     }
-    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
-        int t = item_tile[item];
+    for (int t = R.t0; t <= R.t1; ++t) {
         const TileDesc &T = tiles[t];
-        phase_final<V>(T, item - T.item0, P);
+        int a = max(R.i0, T.item0), b = min(R.i1, T.item0 + T.nitems);
+        for (int item = a; item < b; ++item) phase_final<V>(T, item - T.item0, P);
     }
 }
 
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+/* 2-D map of a stacked plane: dim0 = pitch elements, dim1 = rows */
+static int make_map(CUtensorMap &m, const void *base, size_t esize, int pitch, int rows, int bx,
+                    int by)
+{
+    auto enc = tensor_map_encoder();
+    if (!enc) return fail(CUPHU_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    cuuint64_t dims[2] = {(cuuint64_t)pitch, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)pitch * esize};
+    cuuint32_t box[2] = {(cuuint32_t)bx, (cuuint32_t)by};
+    cuuint32_t es[2] = {1, 1};
+    CUtensorMapDataType dt = esize == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                                        : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    CUresult r = enc(&m, dt, 2, const_cast<void *>(base), dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(CUPHU_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    return 0;
+}
+
 template <typename V>
-static int launch_solve_t(const TileDesc *tiles, const int *item_tile, int nitems,
-                          const SolverPlanes &P, TileState *st, double *part, SolverCtl *ctl,
-                          const SolveParams &sp, long long timeout_ns, int device,
+static int make_maps(SolveMaps &M, const SolverPlanes &P, int pitch, int rows)
+{
+    const size_t v = sizeof(V);
+    int rc = 0;
+    rc |= make_map(M.zA, P.z, v, pitch, rows, kSegW, kItemBy + 2);
+    rc |= make_map(M.p0A, P.p0, v, pitch, rows, kSegW, kItemBy + 2);
+    rc |= make_map(M.p1A, P.p1, v, pitch, rows, kSegW, kItemBy + 2);
+    rc |= make_map(M.wdA, P.wd, 4, pitch, rows, kItemBx, kItemBy + 1);
+    rc |= make_map(M.wrA, P.wr, 4, pitch, rows, kWrW, kItemBy);
+    rc |= make_map(M.xB, P.x, 8, pitch, rows, kItemBx, kItemBy);
+    rc |= make_map(M.p0B, P.p0, v, pitch, rows, kItemBx, kItemBy);
+    rc |= make_map(M.p1B, P.p1, v, pitch, rows, kItemBx, kItemBy);
+    rc |= make_map(M.qB, P.q, v, pitch, rows, kItemBx, kItemBy);
+    rc |= make_map(M.rB, P.r, v, pitch, rows, kItemBx, kItemBy);
+    rc |= make_map(M.dB, P.diag, v, pitch, rows, kItemBx, kItemBy);
+    return rc ? CUPHU_ERR_CUDA : 0;
+}
+
+template <typename V>
+static int launch_solve_t(const TileDesc *tiles, const int *item_tile, int nitems, int ntiles,
+                          const SolverPlanes &P, int pitch, int rows, TileState *st, double *part,
+                          SolverCtl *ctl, const SolveParams &sp, long long timeout_ns, int device,
                           cudaStream_t s)
 {
+    SolveMaps M;
+    int rcm = make_maps<V>(M, P, pitch, rows);
+    if (rcm) return rcm;
     int nsm = 0, per_sm = 0;
     CUPHU_TRY_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+    const size_t smem = solve_smem_bytes<V>();
+    CUPHU_TRY_CUDA(cudaFuncSetAttribute(k_solve<V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem));
     CUPHU_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve<V>,
-                                                                 kItemThreads, 0));
+                                                                 kItemThreads, smem));
     if (per_sm < 1) return fail(CUPHU_ERR_CUDA, "solver kernel cannot be resident");
     int grid = std::min(nsm * per_sm, std::max(nitems, 1));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(kItemThreads);
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    CUPHU_TRY_CUDA(cudaLaunchKernelEx(&cfg, k_solve<V>, tiles, item_tile, nitems, P, st, part,
-                                      ctl, sp, timeout_ns));
+    CUPHU_TRY_CUDA(cudaLaunchKernelEx(&cfg, k_solve<V>, tiles, item_tile, nitems, ntiles, P, st,
+                                      part, ctl, sp, timeout_ns, M));
     return 0;
 }
 
 int launch_solve(bool fp64, const TileDesc *tiles, const int *item_tile, int nitems,
-                 int ntiles, const SolverPlanes &P, TileState *st, double *part,
-                 SolverCtl *ctl, const SolveParams &sp, int device, cudaStream_t s)
+                 int ntiles, const SolverPlanes &P, int plane_pitch, int plane_rows,
+                 TileState *st, double *part, SolverCtl *ctl, const SolveParams &sp,
+                 int device, cudaStream_t s)
 {
-    (void)ntiles;
     long long timeout_ns = sp.timeout_ns;
     if (fp64)
-        return launch_solve_t<double>(tiles, item_tile, nitems, P, st, part, ctl, sp,
-                                      timeout_ns, device, s);
-    return launch_solve_t<float>(tiles, item_tile, nitems, P, st, part, ctl, sp, timeout_ns,
-                                 device, s);
+        return launch_solve_t<double>(tiles, item_tile, nitems, ntiles, P, plane_pitch, plane_rows,
+                                      st, part, ctl, sp, timeout_ns, device, s);
+    return launch_solve_t<float>(tiles, item_tile, nitems, ntiles, P, plane_pitch, plane_rows, st,
+                                 part, ctl, sp, timeout_ns, device, s);
 }
 
 }  // namespace cuphu

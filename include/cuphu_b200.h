@@ -138,6 +138,7 @@ typedef struct CuPhuSolveStats {
     int    max_iters_pass;    /* largest per-pass iteration count                */
     double solve_ms;          /* device time of the persistent solve            */
     double total_ms;          /* device time of the whole GPU pipeline          */
+    double px_iters;          /* sum over tiles and passes of iterations x pixels */
 } CuPhuSolveStats;
 
 /* ── defaults (ref cuphu.h:177-179) ─────────────────────────────────────── */
