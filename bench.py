@@ -103,11 +103,11 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_scene(workload, seed):
+def make_scene(workload, seed, scale=None):
     from cuphu_b200 import synthetic as S
     name = {"c2_8192_topo": "c2_8192_topo", "c1_4096_smooth": "c1_4096_smooth",
             "c0_512_defo": "c0_512_defo", "c4_2048_defo": "c4_2048_defo"}[workload]
-    ig, g, truth, ex = S.config_scene(name, seed=seed)
+    ig, g, truth, ex = S.config_scene(name, seed=seed, scale=scale)
     return ig, g, ex
 
 
@@ -165,7 +165,7 @@ def run_ours(args, rank, world, local_rank):
                                  default_tile_params, lib)
     torch.cuda.set_device(local_rank)
     L = lib()
-    ig, g, ex = make_scene(args.workload, args.seed + rank * 0)
+    ig, g, ex = make_scene(args.workload, args.seed, args.scale)
     nrow, ncol = g.shape
     npix = nrow * ncol
     mode = {"smooth": 0, "defo": 1, "topo": 2}[ex["cost"]]
@@ -367,6 +367,8 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--scale", type=int, default=None,
+                    help="edge length override of the workload (small profiling cases)")
     ap.add_argument("--profile", action="store_true",
                     help="warm-up + one device step only (for ncu captures)")
     args = ap.parse_args()

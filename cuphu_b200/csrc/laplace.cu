@@ -98,6 +98,22 @@ __device__ __forceinline__ void store_partial(double acc, double *part, int item
     if (threadIdx.x == 0) part[item] = bs;
 }
 
+/* block tree without the leading barrier, for item loops that already
+ * separate consecutive uses of sw; returns after the barrier that follows
+ * the warp sums, so every thread has finished the caller's work on the item */
+__device__ __forceinline__ double block_sum_item(double v, double *sw)
+{
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sw[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        v = lane < (int)(blockDim.x >> 5) ? sw[lane] : 0.0;
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    }
+    return v;
+}
+
 __device__ __forceinline__ unsigned long long globaltimer()
 {
     unsigned long long t;
@@ -376,25 +392,29 @@ __device__ __forceinline__ void issue_a(const TileDesc &T, int li, const SolveMa
 }
 
 /* stencil pass on a staged item: p_new = z + beta p_old (own + halo ring),
- * q = A p_new, partial p.q */
+ * q = A p_new, thread partial of p.q (FP64 accumulation).  FP64 mode: FP64
+ * arithmetic in the oracle's operation order.  Mixed mode: FP32 arithmetic
+ * (the SpMV and vector update), FP64 only for the dot. */
 template <typename V>
 __device__ double compute_a(const TileDesc &T, int li, const SolverPlanes &P, V *pnew_all,
                             bool first, double beta, const char *stage, V *Pn)
 {
+    constexpr bool F32 = sizeof(V) == 4;
     const int r0b = (li / T.nbx) * kItemBy, c0b = (li % T.nbx) * kItemBx;
     const V *Z = (const V *)stage;
     const V *PO = (const V *)(stage + StageA<V>::kVec);
     const float *WD = (const float *)(stage + 2 * StageA<V>::kVec);
     const float *WR = (const float *)(stage + 2 * StageA<V>::kVec + StageA<V>::kWd);
     const int nr = T.nr, nc = T.nc;
+    const float betaf = (float)beta;
     for (int k = threadIdx.x; k < kHaloH * kHaloW; k += blockDim.x) {
         int i = k / kHaloW, j = k % kHaloW;
         int gr = r0b - 1 + i, gc = c0b - 1 + j;
         V v = (V)0;
         if (gr >= 0 && gr < nr && gc >= 0 && gc < nc) {
             int sidx = i * kSegW + j + 3;
-            double z = (double)Z[sidx];
-            v = (V)(first ? z : __fma_rn(beta, (double)PO[sidx], z));
+            if (F32) v = first ? Z[sidx] : (V)__fmaf_rn(betaf, (float)PO[sidx], (float)Z[sidx]);
+            else v = first ? Z[sidx] : (V)__fma_rn(beta, (double)PO[sidx], (double)Z[sidx]);
         }
         Pn[k] = v;
     }
@@ -404,21 +424,30 @@ __device__ double compute_a(const TileDesc &T, int li, const SolverPlanes &P, V 
     double acc = 0.0;
     if (r < nr && c0 < nc) {
         V pn[4] = {(V)0, (V)0, (V)0, (V)0}, qv[4] = {(V)0, (V)0, (V)0, (V)0};
-        const double eps = (double)kLapEpsF;
 #pragma unroll
         for (int j = 0; j < kItemVx; ++j) {
             int c = c0 + j;
             if (c >= nc) continue;
             int s = (ty + 1) * kHaloW + tx * kItemVx + j + 1;
-            pn[j] = Pn[s];
-            double xa = (double)pn[j];
-            double y = eps * xa;
             int wc = tx * kItemVx + j;
-            if (r < nr - 1) y = __fma_rn((double)WD[(ty + 1) * kItemBx + wc], xa - (double)Pn[s + kHaloW], y);
-            if (r > 0)      y = __fma_rn((double)WD[ty * kItemBx + wc], xa - (double)Pn[s - kHaloW], y);
-            if (c < nc - 1) y = __fma_rn((double)WR[ty * kWrW + wc + 4], xa - (double)Pn[s + 1], y);
-            if (c > 0)      y = __fma_rn((double)WR[ty * kWrW + wc + 3], xa - (double)Pn[s - 1], y);
-            qv[j] = (V)y;
+            pn[j] = Pn[s];
+            if (F32) {
+                float xa = (float)pn[j];
+                float y = __fmul_rn(kLapEpsF, xa);
+                if (r < nr - 1) y = __fmaf_rn(WD[(ty + 1) * kItemBx + wc], xa - (float)Pn[s + kHaloW], y);
+                if (r > 0)      y = __fmaf_rn(WD[ty * kItemBx + wc], xa - (float)Pn[s - kHaloW], y);
+                if (c < nc - 1) y = __fmaf_rn(WR[ty * kWrW + wc + 4], xa - (float)Pn[s + 1], y);
+                if (c > 0)      y = __fmaf_rn(WR[ty * kWrW + wc + 3], xa - (float)Pn[s - 1], y);
+                qv[j] = (V)y;
+            } else {
+                double xa = (double)pn[j];
+                double y = (double)kLapEpsF * xa;
+                if (r < nr - 1) y = __fma_rn((double)WD[(ty + 1) * kItemBx + wc], xa - (double)Pn[s + kHaloW], y);
+                if (r > 0)      y = __fma_rn((double)WD[ty * kItemBx + wc], xa - (double)Pn[s - kHaloW], y);
+                if (c < nc - 1) y = __fma_rn((double)WR[ty * kWrW + wc + 4], xa - (double)Pn[s + 1], y);
+                if (c > 0)      y = __fma_rn((double)WR[ty * kWrW + wc + 3], xa - (double)Pn[s - 1], y);
+                qv[j] = (V)y;
+            }
             acc = __fma_rn((double)pn[j], (double)qv[j], acc);
         }
         size_t o = T.pix + (size_t)r * T.pitch + c0;
@@ -474,11 +503,19 @@ __device__ double compute_b(const TileDesc &T, int li, const SolverPlanes &P, do
         if (c0 + j >= T.nc) continue;
         xv[j] = __fma_rn(alpha, (double)PB[s0 + j], xv[j]);
         if (update_r) {
-            V rn = (V)__fma_rn(-alpha, (double)QB[s0 + j], (double)rv[j]);
-            rv[j] = rn;
-            double z = (double)rn / (double)DB[s0 + j];
-            zv[j] = (V)z;
-            acc = __fma_rn((double)rn, z, acc);
+            if (sizeof(V) == 4) {
+                float rn = __fmaf_rn(-(float)alpha, (float)QB[s0 + j], (float)rv[j]);
+                float z = __fdiv_rn(rn, (float)DB[s0 + j]);
+                rv[j] = (V)rn;
+                zv[j] = (V)z;
+                acc = __fma_rn((double)rn, (double)z, acc);
+            } else {
+                V rn = (V)__fma_rn(-alpha, (double)QB[s0 + j], (double)rv[j]);
+                rv[j] = rn;
+                double z = (double)rn / (double)DB[s0 + j];
+                zv[j] = (V)z;
+                acc = __fma_rn((double)rn, z, acc);
+            }
         }
     }
     size_t o = T.pix + (size_t)r * T.pitch + c0;
@@ -488,88 +525,6 @@ __device__ double compute_b(const TileDesc &T, int li, const SolverPlanes &P, do
         st4((V *)P.z + o, zv);
     }
     return acc;
-}
-
-__device__ __forceinline__ int next_active_item(int item, int i1, const int *item_tile,
-                                                const TileDesc *tiles, const TileState *st)
-{
-    while (item < i1) {
-        int t = item_tile[item];
-        if (__ldcg(&st[t].active)) return item;
-        item = tiles[t].item0 + tiles[t].nitems;
-    }
-    return i1;
-}
-
-/* NS-stage ring of a block */
-struct Pipe {
-    char *stage[4];
-    uint64_t *bar;
-    uint32_t uses[4];
-    int ns;
-};
-
-/* run a staged pass over this block's items of active tiles.  KIND 0: the
- * stencil pass, KIND 1: the update pass */
-template <int KIND, typename V>
-__device__ void run_pass(const TileDesc *tiles, const int *item_tile, int i0, int i1,
-                         const SolverPlanes &P, const SolveMaps &M, const TileState *st,
-                         int psel, V *pvec, bool flag, double *part, double *sw, V *Pn, Pipe &pp,
-                         SolverCtl *ctl, long long timeout_ns)
-{
-    int q[4];   /* items in flight, oldest first */
-    int nq = 0;
-    int nxt = next_active_item(i0, i1, item_tile, tiles, st);
-    if (nxt >= i1) return;
-    if (threadIdx.x == 0) {
-        fence_async_global();
-        fence_async_smem();
-    }
-    int issued = 0, done = 0;
-    /* prologue: fill ns - 1 stages */
-    while (nq < pp.ns - 1 && nxt < i1) {
-        if (threadIdx.x == 0) {
-            const TileDesc &T = tiles[item_tile[nxt]];
-            int sidx = issued % pp.ns;
-            if (KIND == 0) issue_a<V>(T, nxt - T.item0, M, psel, flag, pp.stage[sidx], &pp.bar[sidx]);
-            else issue_b<V>(T, nxt - T.item0, M, psel, flag, pp.stage[sidx], &pp.bar[sidx]);
-        }
-        q[nq++] = nxt;
-        ++issued;
-        nxt = next_active_item(nxt + 1, i1, item_tile, tiles, st);
-    }
-    while (nq > 0) {
-        if (nxt < i1) {
-            if (threadIdx.x == 0) {
-                fence_async_smem();
-                const TileDesc &T = tiles[item_tile[nxt]];
-                int sidx = issued % pp.ns;
-                if (KIND == 0) issue_a<V>(T, nxt - T.item0, M, psel, flag, pp.stage[sidx], &pp.bar[sidx]);
-                else issue_b<V>(T, nxt - T.item0, M, psel, flag, pp.stage[sidx], &pp.bar[sidx]);
-            }
-            q[nq++] = nxt;
-            ++issued;
-            nxt = next_active_item(nxt + 1, i1, item_tile, tiles, st);
-        }
-        int cur = q[0];
-        for (int k = 1; k < nq; ++k) q[k - 1] = q[k];
-        --nq;
-        int sidx = done % pp.ns;
-        mbar_wait(&pp.bar[sidx], pp.uses[sidx] & 1u, ctl, timeout_ns);
-        pp.uses[sidx]++;
-        ++done;
-        int t = item_tile[cur];
-        const TileDesc &T = tiles[t];
-        double acc;
-        if (KIND == 0) {
-            acc = compute_a<V>(T, cur - T.item0, P, pvec, flag, __ldcg(&st[t].beta), pp.stage[sidx], Pn);
-            store_partial(acc, part, cur, sw);
-        } else {
-            acc = compute_b<V>(T, cur - T.item0, P, __ldcg(&st[t].alpha), flag, pp.stage[sidx]);
-            if (flag) store_partial(acc, part, cur, sw);
-        }
-        __syncthreads();
-    }
 }
 
 /* ── IRLS reweight (A13): w = w0 / sqrt(e^2 + delta^2) ───────────────────── */
@@ -642,13 +597,219 @@ __device__ void phase_final(const TileDesc &T, int li, const SolverPlanes &P)
         *reinterpret_cast<float4 *>(P.cont + T.pix + prow + q.c0) = make_float4(co[0], co[1], co[2], co[3]);
 }
 
-/* Block b owns the contiguous work-item range [b*n/G, (b+1)*n/G); items are
- * tile-major, so a block touches one or a few consecutive tiles.  The owner
- * of a tile (the block holding its first item) maintains the global count of
- * active tiles. */
-struct Range {
-    int i0, i1, t0, t1;
+/* ── work distribution ─────────────────────────────────────────────────────
+ * At every phase each block takes an equal slice of the items of the tiles
+ * that are still active (tile-major order), so tiles that converge late get
+ * the whole GPU instead of the few blocks that own them.  The active flags
+ * were published before the last grid barrier; every block computes the same
+ * prefix sum of active item counts in shared memory.  Tile scalars are
+ * reduced redundantly (and identically) by every block whose slice touches
+ * the tile; the block whose slice holds the tile's first item is its owner
+ * for the global active-tile count. */
+constexpr int kMaxTiles = 1024;
+constexpr int kCacheTiles = 16;
+
+struct SliceCtl {
+    int pre[kMaxTiles + 1];          /* exclusive prefix of counted item numbers */
+    int s0, s1, t0, t1;              /* my slice in counted order, tiles it spans */
+    int ncached;
+    TileDesc d[kCacheTiles];
+    double alpha[kCacheTiles], beta[kCacheTiles];
+    int active[kCacheTiles];
 };
+
+__device__ __forceinline__ const TileDesc &stile(const SliceCtl &sc, const TileDesc *g, int t)
+{
+    int k = t - sc.t0;
+    return (k >= 0 && k < sc.ncached) ? sc.d[k] : g[t];
+}
+__device__ __forceinline__ int sactive(const SliceCtl &sc, const TileState *st, int t)
+{
+    int k = t - sc.t0;
+    return (k >= 0 && k < sc.ncached) ? sc.active[k] : __ldcg(&st[t].active);
+}
+__device__ __forceinline__ double sbeta(const SliceCtl &sc, const TileState *st, int t)
+{
+    int k = t - sc.t0;
+    return (k >= 0 && k < sc.ncached) ? sc.beta[k] : __ldcg(&st[t].beta);
+}
+__device__ __forceinline__ double salpha(const SliceCtl &sc, const TileState *st, int t)
+{
+    int k = t - sc.t0;
+    return (k >= 0 && k < sc.ncached) ? sc.alpha[k] : __ldcg(&st[t].alpha);
+}
+__device__ __forceinline__ void sput(SliceCtl &sc, int t, const TileState &S)
+{
+    int k = t - sc.t0;
+    if (k >= 0 && k < sc.ncached) {
+        sc.active[k] = S.active;
+        sc.alpha[k] = S.alpha;
+        sc.beta[k] = S.beta;
+    }
+}
+
+/* tile containing counted position p (pre[t] <= p < pre[t+1]) */
+__device__ __forceinline__ int slice_tile(const SliceCtl &sc, int ntiles, int p)
+{
+    int lo = 0, hi = ntiles - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (sc.pre[mid] <= p) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+/* Build the prefix sum of item counts (all tiles, or only the tiles active in
+ * `st`) and this block's slice; caches the descriptors of the slice's tiles
+ * and, with `st`, their scalars. */
+__device__ void setup_slice(SliceCtl &sc, const TileDesc *tiles, const TileState *st,
+                            int ntiles, double *swd)
+{
+    int *sw = reinterpret_cast<int *>(swd);
+    const int per = (ntiles + blockDim.x - 1) / blockDim.x;
+    const int b0 = threadIdx.x * per;
+    int loc = 0;
+    for (int k = 0; k < per; ++k) {
+        int t = b0 + k;
+        if (t < ntiles && (!st || __ldcg(&st[t].active))) loc += tiles[t].nitems;
+    }
+    /* block exclusive scan of loc */
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = loc;
+    for (int off = 1; off < 32; off <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, off);
+        if (lane >= off) x += y;
+    }
+    __syncthreads();
+    if (lane == 31) sw[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int v = lane < (int)(blockDim.x >> 5) ? sw[lane] : 0;
+        for (int off = 1; off < 32; off <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, v, off);
+            if (lane >= off) v += y;
+        }
+        sw[lane] = v;
+    }
+    __syncthreads();
+    int run = x - loc + (w > 0 ? sw[w - 1] : 0);
+    for (int k = 0; k < per; ++k) {
+        int t = b0 + k;
+        if (t < ntiles) {
+            sc.pre[t] = run;
+            if (!st || __ldcg(&st[t].active)) run += tiles[t].nitems;
+        }
+    }
+    if (threadIdx.x == blockDim.x - 1) sc.pre[ntiles] = run;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int total = sc.pre[ntiles];
+        sc.s0 = (int)((long long)blockIdx.x * total / gridDim.x);
+        sc.s1 = (int)((long long)(blockIdx.x + 1) * total / gridDim.x);
+        if (sc.s0 < sc.s1) {
+            sc.t0 = slice_tile(sc, ntiles, sc.s0);
+            sc.t1 = slice_tile(sc, ntiles, sc.s1 - 1);
+        } else {
+            sc.t0 = 0;
+            sc.t1 = -1;
+        }
+        sc.ncached = min(max(sc.t1 - sc.t0 + 1, 0), kCacheTiles);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < sc.ncached; k += blockDim.x) {
+        int t = sc.t0 + k;
+        sc.d[k] = tiles[t];
+        if (st) {
+            sc.active[k] = __ldcg(&st[t].active);
+            sc.alpha[k] = __ldcg(&st[t].alpha);
+            sc.beta[k] = __ldcg(&st[t].beta);
+        }
+    }
+    __syncthreads();
+}
+
+/* this block's items of tile t in counted order: [a, b) of local indices */
+__device__ __forceinline__ void slice_items(const SliceCtl &sc, const TileDesc &T, int t, int &a,
+                                            int &b)
+{
+    a = max(sc.s0, sc.pre[t]) - sc.pre[t];
+    b = min(sc.s1, sc.pre[t] + T.nitems) - sc.pre[t];
+}
+
+/* position in the slice: counted position p, tile t */
+struct Cursor {
+    int p, t;
+};
+
+__device__ __forceinline__ Cursor cursor_active(Cursor c, const SliceCtl &sc, const TileDesc *g,
+                                                const TileState *st, int ntiles)
+{
+    while (c.p < sc.s1) {
+        while (c.t + 1 <= ntiles && sc.pre[c.t + 1] <= c.p) ++c.t;
+        if (sactive(sc, st, c.t)) return c;
+        c.p = sc.pre[c.t + 1];
+    }
+    return c;
+}
+
+/* run a staged pass over this block's slice.  KIND 0: the stencil pass,
+ * KIND 1: the update pass.  NS items are in flight; the stage of item k is
+ * refilled with item k+NS right after the barrier of item k's reduction,
+ * which every thread reaches only after its last read of the stage and Pn. */
+template <int KIND, typename V>
+__device__ void run_pass(const SliceCtl &sc, const TileDesc *gt, const TileState *st, int ntiles,
+                         const SolverPlanes &P, const SolveMaps &M, int psel, V *pvec, bool flag,
+                         double *part, double *sw, V *Pn, char *stages, uint64_t *bars,
+                         uint32_t &parity, SolverCtl *ctl, long long timeout_ns)
+{
+    constexpr int NS = n_stages<V>();
+    constexpr size_t SB = stage_bytes<V>();
+    if (sc.s0 >= sc.s1) return;
+    Cursor ci = cursor_active(Cursor{sc.s0, sc.t0}, sc, gt, st, ntiles);
+    if (ci.p >= sc.s1) return;
+    Cursor cc = ci;
+    if (threadIdx.x == 0) {
+        fence_async_global();
+        fence_async_smem();
+    }
+    for (int k = 0; k < NS && ci.p < sc.s1; ++k) {
+        if (threadIdx.x == 0) {
+            const TileDesc &T = stile(sc, gt, ci.t);
+            int li = ci.p - sc.pre[ci.t];
+            if (KIND == 0) issue_a<V>(T, li, M, psel, flag, stages + k * SB, bars + k);
+            else issue_b<V>(T, li, M, psel, flag, stages + k * SB, bars + k);
+        }
+        ci = cursor_active(Cursor{ci.p + 1, ci.t}, sc, gt, st, ntiles);
+    }
+    int done = 0;
+    while (cc.p < sc.s1) {
+        int s = done % NS;
+        mbar_wait(bars + s, (parity >> s) & 1u, ctl, timeout_ns);
+        parity ^= 1u << s;
+        ++done;
+        const TileDesc &T = stile(sc, gt, cc.t);
+        int li = cc.p - sc.pre[cc.t];
+        double acc;
+        if (KIND == 0)
+            acc = compute_a<V>(T, li, P, pvec, flag, sbeta(sc, st, cc.t), stages + s * SB, Pn);
+        else
+            acc = compute_b<V>(T, li, P, salpha(sc, st, cc.t), flag, stages + s * SB);
+        double bs = block_sum_item(acc, sw);   /* contains the item barrier */
+        if (threadIdx.x == 0) {
+            if (KIND == 0 || flag) part[T.item0 + li] = bs;
+            if (ci.p < sc.s1) {
+                fence_async_smem();
+                const TileDesc &Tn = stile(sc, gt, ci.t);
+                int ln = ci.p - sc.pre[ci.t];
+                if (KIND == 0) issue_a<V>(Tn, ln, M, psel, flag, stages + s * SB, bars + s);
+                else issue_b<V>(Tn, ln, M, psel, flag, stages + s * SB, bars + s);
+            }
+        }
+        if (ci.p < sc.s1) ci = cursor_active(Cursor{ci.p + 1, ci.t}, sc, gt, st, ntiles);
+        cc = cursor_active(Cursor{cc.p + 1, cc.t}, sc, gt, st, ntiles);
+    }
+    __syncthreads();
+}
 
 /* state written by other blocks before the last grid barrier: read from L2 */
 __device__ __forceinline__ TileState load_state(const TileState *p)
@@ -662,16 +823,6 @@ __device__ __forceinline__ TileState load_state(const TileState *p)
     S.active = __ldcg(&p->active);
     S.iter = __ldcg(&p->iter);
     return S;
-}
-
-__device__ __forceinline__ Range block_range(const int *item_tile, int nitems)
-{
-    Range R;
-    R.i0 = (int)((long long)blockIdx.x * nitems / gridDim.x);
-    R.i1 = (int)((long long)(blockIdx.x + 1) * nitems / gridDim.x);
-    R.t0 = R.i0 < R.i1 ? item_tile[R.i0] : 0;
-    R.t1 = R.i0 < R.i1 ? item_tile[R.i1 - 1] : -1;
-    return R;
 }
 
 #ifndef CUPHU_SOLVE_MIN_BLOCKS
@@ -688,47 +839,54 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
     __shared__ double sw[32];
     __shared__ double s_bcast;
     __shared__ __align__(8) uint64_t bars[4];
+    __shared__ SliceCtl sc;
+    constexpr int NS = n_stages<V>();
     char *dsm = (char *)(((uintptr_t)dsm_raw + 127) & ~(uintptr_t)127);
     const bool mixed = sizeof(V) == 4;
     V *pb[2] = {(V *)P.p0, (V *)P.p1};
     double *pbuf[2] = {part, part + nitems};
-    const Range R = block_range(item_tile, nitems);
-    Pipe pp;
-    pp.ns = n_stages<V>();
-    for (int k = 0; k < pp.ns; ++k) {
-        pp.stage[k] = dsm + k * stage_bytes<V>();
-        pp.uses[k] = 0u;
-    }
-    pp.bar = bars;
-    V *Pn = (V *)(dsm + pp.ns * stage_bytes<V>());
+    V *Pn = (V *)(dsm + NS * stage_bytes<V>());
+    uint32_t parity = 0u;
+    (void)item_tile;
     if (threadIdx.x == 0) {
-        for (int k = 0; k < pp.ns; ++k) mbar_init(&bars[k]);
+        for (int k = 0; k < NS; ++k) mbar_init(&bars[k]);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
     int pc = 0;   /* phase counter selecting the partial buffer */
 
     for (int outer = 0; outer <= sp.n_irls; ++outer) {
-        /* assemble b, diag; r = b - A x; partial r.z */
-        for (int t = R.t0; t <= R.t1; ++t) {
-            const TileDesc &T = tiles[t];
-            int a = max(R.i0, T.item0), b = min(R.i1, T.item0 + T.nitems);
-            for (int item = a; item < b; ++item)
-                store_partial(phase_init<V>(T, item - T.item0, P, outer == 0, true),
-                              pbuf[pc & 1], item, sw);
+        /* assemble b, diag; r = b - A x; partial r.z (all tiles) */
+        setup_slice(sc, tiles, nullptr, ntiles, sw);
+        for (int t = sc.t0; t <= sc.t1; ++t) {
+            const TileDesc &T = stile(sc, tiles, t);
+            int a, b;
+            slice_items(sc, T, t, a, b);
+            for (int li = a; li < b; ++li)
+                store_partial(phase_init<V>(T, li, P, outer == 0, true), pbuf[pc & 1],
+                              T.item0 + li, sw);
         }
         ++pc;
         if (!grid_sync(ctl, timeout_ns)) return;
 
+        /* stA: scalars after the stencil-pass decisions, stB: after the
+         * update-pass decisions; each phase reads one and writes the other,
+         * so the active flags a phase slices on never change under it */
+        TileState *stA = st, *stB = st + ntiles;
         int it = 0;
         while (true) {
-            TileState *cur = st + (it & 1) * ntiles;
-            TileState *nxt = st + ((it + 1) & 1) * ntiles;
             V *pnew = pb[(it + 1) & 1];
-            /* reduce r.z of the previous phase and update the tile scalars */
-            for (int t = R.t0; t <= R.t1; ++t) {
-                const TileDesc &T = tiles[t];
-                const bool owner = T.item0 >= R.i0 && T.item0 < R.i1;
+            /* slice over the tiles active in the previous phase; reduce r.z,
+             * update the tile scalars, then the stencil pass */
+            setup_slice(sc, tiles, it == 0 ? nullptr : stB, ntiles, sw);
+            /* tiles not counted this phase keep their inactive flag in stA */
+            if (it > 0 && blockIdx.x == 0)
+                for (int t = threadIdx.x; t < ntiles; t += blockDim.x)
+                    if (!__ldcg(&stB[t].active)) stA[t].active = 0;
+            for (int t = sc.t0; t <= sc.t1; ++t) {
+                const TileDesc &T = stile(sc, tiles, t);
+                if (sc.pre[t + 1] == sc.pre[t]) continue;          /* not counted */
+                const bool owner = sc.pre[t] >= sc.s0 && sc.pre[t] < sc.s1;
                 TileState S;
                 if (it == 0) {
                     double tot = tile_reduce(T, pbuf[(pc - 1) & 1], sw, &s_bcast);
@@ -741,66 +899,75 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
                     S.active = (tot > 0.0 && sp.max_iter > 0) ? 1 : 0;
                     if (owner && threadIdx.x == 0 && S.active) atomicAdd(&ctl->n_active, 1);
                 } else {
-                    S = load_state(cur + t);
-                    if (S.active) {
-                        double tot = tile_reduce(T, pbuf[(pc - 1) & 1], sw, &s_bcast);
-                        S.iter += 1;
-                        if (tot < S.thr || S.iter >= sp.max_iter) {
-                            S.active = 0;
-                            if (owner && threadIdx.x == 0) {
-                                atomicSub(&ctl->n_active, 1);
-                                atomicAdd(&ctl->px_iters, (unsigned long long)S.iter *
-                                                              (unsigned long long)((long long)T.nr * T.nc));
-                            }
-                        } else {
-                            S.beta = tot / S.rz;
-                            S.rz = tot;
+                    S = load_state(stB + t);
+                    double tot = tile_reduce(T, pbuf[(pc - 1) & 1], sw, &s_bcast);
+                    S.iter += 1;
+                    if (tot < S.thr || S.iter >= sp.max_iter) {
+                        S.active = 0;
+                        if (owner && threadIdx.x == 0) {
+                            atomicSub(&ctl->n_active, 1);
+                            atomicAdd(&ctl->px_iters, (unsigned long long)S.iter *
+                                                          (unsigned long long)((long long)T.nr * T.nc));
                         }
+                    } else {
+                        S.beta = tot / S.rz;
+                        S.rz = tot;
                     }
                 }
-                if (threadIdx.x == 0) nxt[t] = S;
+                if (threadIdx.x == 0) {
+                    stA[t] = S;
+                    sput(sc, t, S);
+                }
             }
             __syncthreads();
-            /* stencil pass */
-            run_pass<0, V>(tiles, item_tile, R.i0, R.i1, P, M, nxt, it & 1, pnew, it == 0,
-                           pbuf[pc & 1], sw, Pn, pp, ctl, timeout_ns);
+            run_pass<0, V>(sc, tiles, stA, ntiles, P, M, it & 1, pnew, it == 0, pbuf[pc & 1], sw,
+                           Pn, dsm, bars, parity, ctl, timeout_ns);
             ++pc;
             if (!grid_sync(ctl, timeout_ns)) return;
             if (*(volatile int *)&ctl->snap <= 0) break;
 
-            /* reduce p.q, alpha (pq <= 0 ends the tile's solve) */
+            /* slice over the tiles active in the stencil pass; reduce p.q, alpha */
             const bool repl = mixed && sp.replace_every > 0 && ((it + 1) % sp.replace_every) == 0;
-            for (int t = R.t0; t <= R.t1; ++t) {
-                const TileDesc &T = tiles[t];
-                const bool owner = T.item0 >= R.i0 && T.item0 < R.i1;
-                TileState S = load_state(nxt + t);
-                if (!S.active) continue;
+            setup_slice(sc, tiles, stA, ntiles, sw);
+            if (blockIdx.x == 0)
+                for (int t = threadIdx.x; t < ntiles; t += blockDim.x)
+                    if (!__ldcg(&stA[t].active)) stB[t].active = 0;
+            for (int t = sc.t0; t <= sc.t1; ++t) {
+                const TileDesc &T = stile(sc, tiles, t);
+                if (sc.pre[t + 1] == sc.pre[t]) continue;
+                const bool owner = sc.pre[t] >= sc.s0 && sc.pre[t] < sc.s1;
+                TileState S = load_state(stA + t);
                 double pq = tile_reduce(T, pbuf[(pc - 1) & 1], sw, &s_bcast);
                 if (pq <= 0.0) {
-                    if (threadIdx.x == 0) nxt[t].active = 0;
+                    S.active = 0;
                     if (owner && threadIdx.x == 0) {
                         atomicSub(&ctl->n_active, 1);
                         atomicAdd(&ctl->px_iters, (unsigned long long)S.iter *
                                                       (unsigned long long)((long long)T.nr * T.nc));
                     }
-                } else if (threadIdx.x == 0) {
-                    nxt[t].alpha = S.rz / pq;
+                } else {
+                    S.alpha = S.rz / pq;
+                }
+                if (threadIdx.x == 0) {
+                    stB[t] = S;
+                    sput(sc, t, S);
                 }
             }
             __syncthreads();
-            /* update pass (with periodic true residual in mixed precision) */
-            run_pass<1, V>(tiles, item_tile, R.i0, R.i1, P, M, nxt, (it + 1) & 1, pnew, !repl,
-                           pbuf[pc & 1], sw, Pn, pp, ctl, timeout_ns);
+            run_pass<1, V>(sc, tiles, stB, ntiles, P, M, (it + 1) & 1, pnew, !repl, pbuf[pc & 1],
+                           sw, Pn, dsm, bars, parity, ctl, timeout_ns);
             if (!repl) ++pc;
             if (!grid_sync(ctl, timeout_ns)) return;
             if (repl) {
-                for (int t = R.t0; t <= R.t1; ++t) {
-                    const TileDesc &T = tiles[t];
-                    if (!__ldcg(&nxt[t].active)) continue;
-                    int a = max(R.i0, T.item0), b = min(R.i1, T.item0 + T.nitems);
-                    for (int item = a; item < b; ++item)
-                        store_partial(phase_init<V>(T, item - T.item0, P, false, false),
-                                      pbuf[pc & 1], item, sw);
+                setup_slice(sc, tiles, stB, ntiles, sw);
+                for (int t = sc.t0; t <= sc.t1; ++t) {
+                    const TileDesc &T = stile(sc, tiles, t);
+                    int a, b;
+                    if (sc.pre[t + 1] == sc.pre[t]) continue;
+                    slice_items(sc, T, t, a, b);
+                    for (int li = a; li < b; ++li)
+                        store_partial(phase_init<V>(T, li, P, false, false), pbuf[pc & 1],
+                                      T.item0 + li, sw);
                 }
                 ++pc;
                 if (!grid_sync(ctl, timeout_ns)) return;
@@ -814,18 +981,22 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
         }
         if (outer < sp.n_irls) {
             float delta = sp.deltas[outer];
-            for (int t = R.t0; t <= R.t1; ++t) {
-                const TileDesc &T = tiles[t];
-                int a = max(R.i0, T.item0), b = min(R.i1, T.item0 + T.nitems);
-                for (int item = a; item < b; ++item) phase_rw<V>(T, item - T.item0, P, delta);
+            setup_slice(sc, tiles, nullptr, ntiles, sw);
+            for (int t = sc.t0; t <= sc.t1; ++t) {
+                const TileDesc &T = stile(sc, tiles, t);
+                int a, b;
+                slice_items(sc, T, t, a, b);
+                for (int li = a; li < b; ++li) phase_rw<V>(T, li, P, delta);
             }
             if (!grid_sync(ctl, timeout_ns)) return;
         }
     }
-    for (int t = R.t0; t <= R.t1; ++t) {
-        const TileDesc &T = tiles[t];
-        int a = max(R.i0, T.item0), b = min(R.i1, T.item0 + T.nitems);
-        for (int item = a; item < b; ++item) phase_final<V>(T, item - T.item0, P);
+    setup_slice(sc, tiles, nullptr, ntiles, sw);
+    for (int t = sc.t0; t <= sc.t1; ++t) {
+        const TileDesc &T = stile(sc, tiles, t);
+        int a, b;
+        slice_items(sc, T, t, a, b);
+        for (int li = a; li < b; ++li) phase_final<V>(T, li, P);
     }
 }
 
@@ -889,6 +1060,8 @@ static int launch_solve_t(const TileDesc *tiles, const int *item_tile, int nitem
                           SolverCtl *ctl, const SolveParams &sp, long long timeout_ns, int device,
                           cudaStream_t s)
 {
+    if (ntiles > kMaxTiles)
+        return fail(CUPHU_ERR_INVALID, "at most 1024 tiles per solver launch");
     SolveMaps M;
     int rcm = make_maps<V>(M, P, pitch, rows);
     if (rcm) return rcm;
