@@ -10,7 +10,7 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libcuphu_b200.so")
+LIB_PATH = os.environ.get("CUPHU_B200_LIB", os.path.join(HERE, "lib", "libcuphu_b200.so"))
 
 _D, _L, _I = C.c_double, C.c_long, C.c_int
 

@@ -300,14 +300,23 @@ template <typename V> struct StageB {
     static constexpr uint32_t kTxFull = (uint32_t)(kX + 4 * kV);
     static constexpr uint32_t kTxX = (uint32_t)(kX + kV);
 };
-template <typename V> __host__ __device__ constexpr int n_stages() { return sizeof(V) == 4 ? 3 : 2; }
+#ifndef CUPHU_SOLVE_STAGES_F32
+#define CUPHU_SOLVE_STAGES_F32 2
+#endif
+template <typename V> __host__ __device__ constexpr int n_stages()
+{
+    return sizeof(V) == 4 ? CUPHU_SOLVE_STAGES_F32 : 2;
+}
 template <typename V> __host__ __device__ constexpr size_t stage_bytes()
 {
     return al128(StageA<V>::kBytes > StageB<V>::kBytes ? StageA<V>::kBytes : StageB<V>::kBytes);
 }
+/* p_new of an item with its halo ring, rows of kSegW elements laid out like
+ * the staged boxes (column 0 <-> c0b - 4), so own columns start 16-byte
+ * aligned at column 4 */
 template <typename V> __host__ __device__ constexpr size_t pn_bytes()
 {
-    return al128((size_t)kHaloH * kHaloW * sizeof(V));
+    return al128((size_t)kHaloH * kSegW * sizeof(V));
 }
 template <typename V> __host__ __device__ constexpr size_t solve_smem_bytes()
 {
@@ -391,6 +400,28 @@ __device__ __forceinline__ void issue_a(const TileDesc &T, int li, const SolveMa
     tma_load_2d(WR, &M.wrA, c0b - 4, y, bar);
 }
 
+/* shared-memory vector access of 4 consecutive elements (16-byte aligned) */
+__device__ __forceinline__ void sld4(const float *p, float v[4])
+{
+    float4 t = *reinterpret_cast<const float4 *>(p);
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+__device__ __forceinline__ void sld4(const double *p, double v[4])
+{
+    double2 a = reinterpret_cast<const double2 *>(p)[0];
+    double2 b = reinterpret_cast<const double2 *>(p)[1];
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+
+/* p_new = z + beta p_old: FP32 arithmetic in mixed mode, FP64 in FP64 mode */
+template <typename V>
+__device__ __forceinline__ V pupdate(bool first, double beta, float betaf, V po, V z)
+{
+    if (first) return z;
+    if (sizeof(V) == 4) return (V)__fmaf_rn(betaf, (float)po, (float)z);
+    return (V)__fma_rn(beta, (double)po, (double)z);
+}
+
 /* stencil pass on a staged item: p_new = z + beta p_old (own + halo ring),
  * q = A p_new, thread partial of p.q (FP64 accumulation).  FP64 mode: FP64
  * arithmetic in the oracle's operation order.  Mixed mode: FP32 arithmetic
@@ -399,7 +430,6 @@ template <typename V>
 __device__ double compute_a(const TileDesc &T, int li, const SolverPlanes &P, V *pnew_all,
                             bool first, double beta, const char *stage, V *Pn)
 {
-    constexpr bool F32 = sizeof(V) == 4;
     const int r0b = (li / T.nbx) * kItemBy, c0b = (li % T.nbx) * kItemBx;
     const V *Z = (const V *)stage;
     const V *PO = (const V *)(stage + StageA<V>::kVec);
@@ -407,45 +437,71 @@ __device__ double compute_a(const TileDesc &T, int li, const SolverPlanes &P, V 
     const float *WR = (const float *)(stage + 2 * StageA<V>::kVec + StageA<V>::kWd);
     const int nr = T.nr, nc = T.nc;
     const float betaf = (float)beta;
-    for (int k = threadIdx.x; k < kHaloH * kHaloW; k += blockDim.x) {
-        int i = k / kHaloW, j = k % kHaloW;
-        int gr = r0b - 1 + i, gc = c0b - 1 + j;
-        V v = (V)0;
-        if (gr >= 0 && gr < nr && gc >= 0 && gc < nc) {
-            int sidx = i * kSegW + j + 3;
-            if (F32) v = first ? Z[sidx] : (V)__fmaf_rn(betaf, (float)PO[sidx], (float)Z[sidx]);
-            else v = first ? Z[sidx] : (V)__fma_rn(beta, (double)PO[sidx], (double)Z[sidx]);
-        }
-        Pn[k] = v;
-    }
-    __syncthreads();
     const int ty = threadIdx.x / kItemTx, tx = threadIdx.x % kItemTx;
     const int r = r0b + ty, c0 = c0b + tx * kItemVx;
+    const bool own = r < nr && c0 < nc;
+    /* own p_new: row ty+1, columns 4 + 4 tx .. +3 */
+    V pn[4] = {(V)0, (V)0, (V)0, (V)0};
+    const int so = (ty + 1) * kSegW + 4 + tx * kItemVx;
+    if (own) {
+        V zv[4], pv[4] = {(V)0, (V)0, (V)0, (V)0};
+        sld4(Z + so, zv);
+        if (!first) sld4(PO + so, pv);
+#pragma unroll
+        for (int j = 0; j < kItemVx; ++j)
+            if (c0 + j < nc) pn[j] = pupdate<V>(first, beta, betaf, pv[j], zv[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < kItemVx; ++j) Pn[so + j] = pn[j];
+    /* halo ring: rows above/below (64 each), columns left/right (16 each) */
+    if (threadIdx.x < 2 * kItemBx + 2 * kItemBy) {
+        int h = threadIdx.x, i, jc;
+        if (h < kItemBx) { i = 0; jc = 4 + h; }
+        else if (h < 2 * kItemBx) { i = kItemBy + 1; jc = 4 + h - kItemBx; }
+        else if (h < 2 * kItemBx + kItemBy) { i = 1 + h - 2 * kItemBx; jc = 3; }
+        else { i = 1 + h - 2 * kItemBx - kItemBy; jc = 4 + kItemBx; }
+        int gr = r0b - 1 + i, gc = c0b - 4 + jc;
+        V v = (V)0;
+        if (gr >= 0 && gr < nr && gc >= 0 && gc < nc) {
+            int sidx = i * kSegW + jc;
+            v = pupdate<V>(first, beta, betaf, first ? (V)0 : PO[sidx], Z[sidx]);
+        }
+        Pn[i * kSegW + jc] = v;
+    }
+    __syncthreads();
     double acc = 0.0;
-    if (r < nr && c0 < nc) {
-        V pn[4] = {(V)0, (V)0, (V)0, (V)0}, qv[4] = {(V)0, (V)0, (V)0, (V)0};
+    if (own) {
+        V up[4], dn[4], qv[4] = {(V)0, (V)0, (V)0, (V)0};
+        float wdn[4], wup[4], wrt[4];
+        sld4(Pn + so - kSegW, up);
+        sld4(Pn + so + kSegW, dn);
+        V lf = Pn[so - 1], rt = Pn[so + 4];
+        sld4(WD + (ty + 1) * kItemBx + tx * kItemVx, wdn);
+        sld4(WD + ty * kItemBx + tx * kItemVx, wup);
+        sld4(WR + ty * kWrW + tx * kItemVx + 4, wrt);
+        float wlf = WR[ty * kWrW + tx * kItemVx + 3];
 #pragma unroll
         for (int j = 0; j < kItemVx; ++j) {
             int c = c0 + j;
             if (c >= nc) continue;
-            int s = (ty + 1) * kHaloW + tx * kItemVx + j + 1;
-            int wc = tx * kItemVx + j;
-            pn[j] = Pn[s];
-            if (F32) {
+            V xl = j == 0 ? lf : pn[j - 1];
+            V xr = j == kItemVx - 1 ? rt : pn[j + 1];
+            float wl = j == 0 ? wlf : wrt[j - 1];
+            if (sizeof(V) == 4) {
                 float xa = (float)pn[j];
                 float y = __fmul_rn(kLapEpsF, xa);
-                if (r < nr - 1) y = __fmaf_rn(WD[(ty + 1) * kItemBx + wc], xa - (float)Pn[s + kHaloW], y);
-                if (r > 0)      y = __fmaf_rn(WD[ty * kItemBx + wc], xa - (float)Pn[s - kHaloW], y);
-                if (c < nc - 1) y = __fmaf_rn(WR[ty * kWrW + wc + 4], xa - (float)Pn[s + 1], y);
-                if (c > 0)      y = __fmaf_rn(WR[ty * kWrW + wc + 3], xa - (float)Pn[s - 1], y);
+                if (r < nr - 1) y = __fmaf_rn(wdn[j], xa - (float)dn[j], y);
+                if (r > 0)      y = __fmaf_rn(wup[j], xa - (float)up[j], y);
+                if (c < nc - 1) y = __fmaf_rn(wrt[j], xa - (float)xr, y);
+                if (c > 0)      y = __fmaf_rn(wl, xa - (float)xl, y);
                 qv[j] = (V)y;
             } else {
                 double xa = (double)pn[j];
                 double y = (double)kLapEpsF * xa;
-                if (r < nr - 1) y = __fma_rn((double)WD[(ty + 1) * kItemBx + wc], xa - (double)Pn[s + kHaloW], y);
-                if (r > 0)      y = __fma_rn((double)WD[ty * kItemBx + wc], xa - (double)Pn[s - kHaloW], y);
-                if (c < nc - 1) y = __fma_rn((double)WR[ty * kWrW + wc + 4], xa - (double)Pn[s + 1], y);
-                if (c > 0)      y = __fma_rn((double)WR[ty * kWrW + wc + 3], xa - (double)Pn[s - 1], y);
+                if (r < nr - 1) y = __fma_rn((double)wdn[j], xa - (double)dn[j], y);
+                if (r > 0)      y = __fma_rn((double)wup[j], xa - (double)up[j], y);
+                if (c < nc - 1) y = __fma_rn((double)wrt[j], xa - (double)xr, y);
+                if (c > 0)      y = __fma_rn((double)wl, xa - (double)xl, y);
                 qv[j] = (V)y;
             }
             acc = __fma_rn((double)pn[j], (double)qv[j], acc);
@@ -493,26 +549,31 @@ __device__ double compute_b(const TileDesc &T, int li, const SolverPlanes &P, do
     if (r >= T.nr || c0 >= T.nc) return 0.0;
     const int s0 = ty * kItemBx + tx * kItemVx;
     double xv[4];
-    V rv[4], zv[4];
+    V pv[4], qv[4], rv[4] = {(V)0, (V)0, (V)0, (V)0}, dv[4], zv[4] = {(V)0, (V)0, (V)0, (V)0};
+    sld4(X + s0, xv);
+    sld4(PB + s0, pv);
+    if (update_r) {
+        sld4(QB + s0, qv);
+        sld4(RB + s0, rv);
+        sld4(DB + s0, dv);
+    }
+    const float alphaf = (float)alpha;
     double acc = 0.0;
 #pragma unroll
     for (int j = 0; j < kItemVx; ++j) {
-        xv[j] = X[s0 + j];
-        rv[j] = update_r ? RB[s0 + j] : (V)0;
-        zv[j] = (V)0;
         if (c0 + j >= T.nc) continue;
-        xv[j] = __fma_rn(alpha, (double)PB[s0 + j], xv[j]);
+        xv[j] = __fma_rn(alpha, (double)pv[j], xv[j]);
         if (update_r) {
             if (sizeof(V) == 4) {
-                float rn = __fmaf_rn(-(float)alpha, (float)QB[s0 + j], (float)rv[j]);
-                float z = __fdiv_rn(rn, (float)DB[s0 + j]);
+                float rn = __fmaf_rn(-alphaf, (float)qv[j], (float)rv[j]);
+                float z = __fdiv_rn(rn, (float)dv[j]);
                 rv[j] = (V)rn;
                 zv[j] = (V)z;
                 acc = __fma_rn((double)rn, (double)z, acc);
             } else {
-                V rn = (V)__fma_rn(-alpha, (double)QB[s0 + j], (double)rv[j]);
+                V rn = (V)__fma_rn(-alpha, (double)qv[j], (double)rv[j]);
                 rv[j] = rn;
-                double z = (double)rn / (double)DB[s0 + j];
+                double z = (double)rn / (double)dv[j];
                 zv[j] = (V)z;
                 acc = __fma_rn((double)rn, z, acc);
             }
@@ -826,7 +887,7 @@ __device__ __forceinline__ TileState load_state(const TileState *p)
 }
 
 #ifndef CUPHU_SOLVE_MIN_BLOCKS
-#define CUPHU_SOLVE_MIN_BLOCKS 2
+#define CUPHU_SOLVE_MIN_BLOCKS 3
 #endif
 
 template <typename V>
