@@ -75,6 +75,10 @@ __device__ __forceinline__ float sane(float v) { return isfinite(v) ? v : 0.0f; 
 struct CostConsts {
     double rho0, thresh, rhopow, sigsqrhoconst, sigsqcorr, nsc, nsc2, costscale, defomax;
     int sigsqshortmin;
+    float rhopow_f;   /* screening exponent of the FP32 pow estimate */
+    double screen;    /* relative half-width of the screening interval */
+    float screen_f, sig_f, corr_f, scale_f;   /* FP32 screening constants */
+    int dzmax;        /* DEFO discontinuity shelf in short-cycle steps */
 };
 
 CostConsts make_cost_consts(const CuPhuParams &p);

@@ -40,6 +40,17 @@ CostConsts make_cost_consts(const CuPhuParams &p)
     k.costscale = p.costscale;
     k.defomax = p.defomax;
     k.sigsqshortmin = (int)p.sigsqshortmin;
+    k.rhopow_f = (float)k.rhopow;
+    k.screen = 1e-5 * (1.0 + std::fabs(k.rhopow));
+    k.screen_f = (float)(k.screen + 2e-6);
+    k.sig_f = (float)k.sigsqrhoconst;
+    k.corr_f = (float)k.sigsqcorr;
+    k.scale_f = (float)(k.nsc2 / k.costscale);
+    /* dzmax = clamp(rn(nsc*defomax), 1, 32767) (cuphu_cost.cu:250-251) is a
+     * per-launch constant; the FP64 product is exact as on the device */
+    double dz = std::nearbyint(k.nsc * k.defomax);
+    int dzi = (dz != dz) ? 0 : (dz >= 2147483647.0 ? 2147483647 : (dz <= -2147483648.0 ? (int)-2147483647 - 1 : (int)dz));
+    k.dzmax = std::max(1, std::min(dzi, 32767));
     return k;
 }
 
@@ -83,15 +94,59 @@ struct ArcCost {
     short off, sigsq, dzmax, laycost;
 };
 
+/* hardware 2^x (MUFU EX2, 2 ulp) */
+__device__ __forceinline__ float ex2_approx(float x)
+{
+    float y;
+    asm("ex2.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+/* (int)sigsq_f of the reference (cuphu_cost.cu:109-117) for a coherence rho
+ * already thresholded.  The FP64 pow dominates the kernel's cost, and only
+ * the truncated value matters, so it is screened first with an FP32 pow
+ * estimate through the reference's FP64 formula; whenever the interval of
+ * +-1e-5 (1 + |rhopow|) relative around it (40x the estimate's error bound)
+ * contains no integer the truncated result is certain.  Everything else (intervals that straddle an integer,
+ * bases outside (0,1], non-positive weights) takes the exact FP64 path, so
+ * the result is bit-identical to the reference arithmetic. */
+__device__ __forceinline__ int trunc_sigsq(double rho, short w, const CostConsts &k)
+{
+    double b = 1.0 - rho;
+    if (w > 0 && b > 0.0 && b <= 1.0) {
+        /* MUFU log2/exp2 (|error of log2| <= 2^-22 abs on [0.5,2], 2 ulp
+         * elsewhere; exp2 2 ulp) and FP32 arithmetic (< 6 ulp): the relative
+         * error of v stays below 3e-7 (1 + |rhopow|) + 1e-6; the screen keeps
+         * a >= 10x margin */
+        float pw = ex2_approx(k.rhopow_f * __log2f((float)b));
+        float v = __fmaf_rn(k.sig_f, pw, k.corr_f) * k.scale_f;
+        if (w != 1) v = __fdiv_rn(v, (float)w);
+        float m = __fmaf_rn(k.screen_f, v, 1e-6f);
+        float lo = floorf(v - m);
+        if (lo == floorf(v + m) && lo >= 0.0f && v + m < 1.0e7f) return (int)lo;
+    }
+    double sigsqrho = __dmul_rn(__fma_rn(k.sigsqrhoconst, pow(b, k.rhopow), k.sigsqcorr), k.nsc2);
+    return (int)(sigsqrho / (k.costscale * (double)w));
+}
+
 __device__ __forceinline__ int sigsq_of(double ca, double cb, short w, const CostConsts &k)
 {
     double rho = 0.5 * (ca + cb);
     if (rho < k.thresh) rho = 0.0;
-    double sigsqrho = __dmul_rn(__fma_rn(k.sigsqrhoconst, pow(1.0 - rho, k.rhopow), k.sigsqcorr),
-                                k.nsc2);
-    double sigsq_f = sigsqrho / (k.costscale * (double)w);
-    int s = (int)sigsq_f;
+    int s = trunc_sigsq(rho, w, k);
     if (s < k.sigsqshortmin) s = k.sigsqshortmin;
+    return s;
+}
+
+/* (int)sqrt((double)n) of the reference: floor(sqrt(n)) for n >= 0 (a
+ * correctly rounded FP64 sqrt never crosses an integer for n < 2^52), and
+ * NaN -> 0 for a negative (wrapped) product.  FP32 estimate, exact fix-up. */
+__device__ __forceinline__ int isqrt_floor(int n)
+{
+    if (n <= 0) return 0;
+    int s = (int)sqrtf((float)n);
+    while ((long long)s * s > n) --s;
+    while ((long long)(s + 1) * (s + 1) <= n) ++s;
     return s;
 }
 
@@ -107,19 +162,15 @@ __device__ __forceinline__ ArcCost arc_cost(double ca, double cb, float dpsi, fl
     }
     double rho = 0.5 * (ca + cb);
     if (rho < k.thresh) rho = 0.0;
-    double sigsqrho = __dmul_rn(__fma_rn(k.sigsqrhoconst, pow(1.0 - rho, k.rhopow), k.sigsqcorr),
-                                k.nsc2);
     double dp = (double)dpsi, av = (double)avg;
     double offset = __dmul_rn(k.nsc, __dsub_rn(dp, rho > 0 ? av : __dmul_rn(0.5, av)));
-    double sigsq_f = sigsqrho / (k.costscale * (double)w);
-    int sigsq_i = (int)sigsq_f;
+    int sigsq_i = trunc_sigsq(rho, w, k);
     if (sigsq_i < k.sigsqshortmin) sigsq_i = k.sigsqshortmin;
     int off_i;
     int dzmax = 0, laycost = 0;
     if (DEFO) {
-        dzmax = __double2int_rn(__dmul_rn(k.nsc, k.defomax));
-        dzmax = max(1, min(dzmax, (int)SHRT_MAX));
-        laycost = (int)sqrt((double)(dzmax * sigsq_i));
+        dzmax = k.dzmax;
+        laycost = isqrt_floor(dzmax * sigsq_i);   /* (int)sqrt((double)n), n < 0 -> 0 */
         laycost = min(laycost, (int)SHRT_MAX);
         off_i = __double2int_rn(offset);
     } else {
@@ -137,11 +188,15 @@ __device__ __forceinline__ ArcCost arc_cost(double ca, double cb, float dpsi, fl
  * Block = 256 threads producing a kCostBy x kCostBx block of arcs of one
  * family.  family 0 = row arcs (r,c)->(r+1,c), azimuth diffs, array
  * (nrow-1) x ncol, window (kpar/2 rows, kperp/2 cols); family 1 = col arcs
- * (r,c)->(r,c+1), range diffs, nrow x (ncol-1), window (kperp/2, kpar/2). */
-constexpr int kCostBx = 32;
-constexpr int kCostBy = 16;
+ * (r,c)->(r,c+1), range diffs, nrow x (ncol-1), window (kperp/2, kpar/2).
+ * Interior blocks stage the phase window in shared memory with coalesced
+ * loads and form the differences from it; blocks whose window crosses the
+ * array edge read the mirror-reflected phase directly.  KR/KC > 0 fix the
+ * half windows at compile time (the default 7x7 window); 0 = runtime. */
+constexpr int kCostBx = 64;
+constexpr int kCostBy = 32;
 
-template <bool DEFO>
+template <bool DEFO, int KR0, int KC0>
 __global__ void __launch_bounds__(256) k_costs(const float *__restrict__ ph,
                                                const float *__restrict__ corr,
                                                const short *__restrict__ weights, int nrow,
@@ -156,36 +211,57 @@ __global__ void __launch_bounds__(256) k_costs(const float *__restrict__ ph,
     if (b < nbx0 * nby0) { fam = 0; by = b / nbx0; bx = b % nbx0; }
     else { b -= nbx0 * nby0; fam = 1; by = b / nbx1; bx = b % nbx1; }
 
-    int dr = fam == 0 ? nrow - 1 : nrow;      /* diff array rows */
-    int dc = fam == 0 ? ncol : ncol - 1;      /* diff array cols */
-    int kr = fam == 0 ? kpar / 2 : kperp / 2;
-    int kc = fam == 0 ? kperp / 2 : kpar / 2;
-    int wr = 2 * kr + 1, wc = 2 * kc + 1;
-    int pr = kCostBy + 2 * kr, pc = kCostBx + 2 * kc;
+    const int dr = fam == 0 ? nrow - 1 : nrow;      /* diff array rows */
+    const int dc = fam == 0 ? ncol : ncol - 1;      /* diff array cols */
+    /* with a compile-time square window both families share kr == kc */
+    const int kr = KR0 > 0 ? KR0 : (fam == 0 ? kpar / 2 : kperp / 2);
+    const int kc = KC0 > 0 ? KC0 : (fam == 0 ? kperp / 2 : kpar / 2);
+    const int wr = 2 * kr + 1, wc = 2 * kc + 1;
+    const int pr = kCostBy + 2 * kr, pc = kCostBx + 2 * kc;
     float *D = sm;                 /* pr x pc padded diffs          */
     float *T = sm + pr * pc;       /* pr x kCostBx row-pass results */
-    int r0 = by * kCostBy, c0 = bx * kCostBx;
-
-    /* stage the mirror-padded wrapped differences (cycles) */
-    for (int i = threadIdx.x; i < pr * pc; i += blockDim.x) {
-        int ii = i / pc, jj = i % pc;
-        int sr = reflect_index(r0 + ii - kr, dr);
-        int sc = reflect_index(c0 + jj - kc, dc);
-        float d;
-        if (fam == 0)
-            d = __fdiv_rn(ph[(size_t)sr * ncol + sc] - ph[(size_t)(sr + 1) * ncol + sc], kTwoPiF);
-        else
-            d = __fdiv_rn(ph[(size_t)sr * ncol + sc + 1] - ph[(size_t)sr * ncol + sc], kTwoPiF);
-        D[i] = wrap_cycles(d);
+    float *PH = T + pr * kCostBx;  /* phase window (interior blocks) */
+    const int r0 = by * kCostBy, c0 = bx * kCostBx;
+    const bool interior = r0 - kr >= 0 && r0 + kCostBy + kr <= dr && c0 - kc >= 0 &&
+                          c0 + kCostBx + kc <= dc;
+    if (interior) {
+        /* phase window: family 0 needs pr+1 rows x pc cols, family 1 pr x pc+1 */
+        const int hr = pr + (fam == 0 ? 1 : 0), hc = pc + (fam == 1 ? 1 : 0);
+        const int pr0 = r0 - kr, pc0 = c0 - kc;
+        for (int i = threadIdx.x; i < hr * hc; i += blockDim.x) {
+            int ii = i / hc, jj = i - ii * hc;
+            PH[i] = ph[(size_t)(pr0 + ii) * ncol + pc0 + jj];
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < pr * pc; i += blockDim.x) {
+            int ii = i / pc, jj = i - ii * pc;
+            float d;
+            if (fam == 0) d = __fdiv_rn(PH[ii * hc + jj] - PH[(ii + 1) * hc + jj], kTwoPiF);
+            else d = __fdiv_rn(PH[ii * hc + jj + 1] - PH[ii * hc + jj], kTwoPiF);
+            D[i] = wrap_cycles(d);
+        }
+    } else {
+        for (int i = threadIdx.x; i < pr * pc; i += blockDim.x) {
+            int ii = i / pc, jj = i - ii * pc;
+            int sr = reflect_index(r0 + ii - kr, dr);
+            int sc = reflect_index(c0 + jj - kc, dc);
+            float d;
+            if (fam == 0)
+                d = __fdiv_rn(ph[(size_t)sr * ncol + sc] - ph[(size_t)(sr + 1) * ncol + sc], kTwoPiF);
+            else
+                d = __fdiv_rn(ph[(size_t)sr * ncol + sc + 1] - ph[(size_t)sr * ncol + sc], kTwoPiF);
+            D[i] = wrap_cycles(d);
+        }
     }
     __syncthreads();
     /* row pass: sum k = 0..wc-1 ascending, then divide (cuphu_util.cu:116-121) */
+    const float fwc = (float)wc, fwr = (float)wr;
     for (int i = threadIdx.x; i < pr * kCostBx; i += blockDim.x) {
         int ii = i / kCostBx, jj = i % kCostBx;
         const float *row = D + ii * pc + jj;
         float s = 0.0f;
         for (int q = 0; q < wc; ++q) s = __fadd_rn(s, row[q]);
-        T[i] = __fdiv_rn(s, (float)wc);
+        T[i] = __fdiv_rn(s, fwc);
     }
     __syncthreads();
     size_t nra = (size_t)(nrow - 1) * ncol;
@@ -196,7 +272,7 @@ __global__ void __launch_bounds__(256) k_costs(const float *__restrict__ ph,
         /* column pass (cuphu_util.cu:143-147) */
         float s = 0.0f;
         for (int q = 0; q < wr; ++q) s = __fadd_rn(s, T[(ii + q) * kCostBx + jj]);
-        float avg = __fdiv_rn(s, (float)wr);
+        float avg = __fdiv_rn(s, fwr);
         float dpsi = D[(ii + kr) * pc + jj + kc];
         size_t a;
         float ca, cb;
@@ -343,6 +419,19 @@ int launch_phase_split(const float *re, const float *im, float *ph, long long n,
     return cuda_fail(cudaGetLastError(), "k_phase_split");
 }
 
+template <bool DEFO, int KR, int KC>
+static void launch_costs_t(int nblocks, size_t shm, cudaStream_t s, const float *ph,
+                           const float *corr, const short *weights, int nrow, int ncol, int kperp,
+                           int kpar, const CostConsts &k, void *costs, signed char *res, int nbx0,
+                           int nby0, int nbx1)
+{
+    if (shm > 48 * 1024)
+        cudaFuncSetAttribute(k_costs<DEFO, KR, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)shm);
+    k_costs<DEFO, KR, KC><<<nblocks, 256, shm, s>>>(ph, corr, weights, nrow, ncol, kperp, kpar, k,
+                                                    costs, res, nbx0, nby0, nbx1);
+}
+
 int launch_costs(const float *ph, const float *corr, const short *weights, int nrow, int ncol,
                  int mode, const CuPhuParams &p, void *costs, signed char *res, cudaStream_t s)
 {
@@ -358,20 +447,15 @@ int launch_costs(const float *ph, const float *corr, const short *weights, int n
     int nblocks = nbx0 * nby0 + nbx1 * nby1;
     if (nblocks == 0) return 0;
     int kmax = std::max(kperp / 2, kpar / 2);
-    size_t shm = ((size_t)(kCostBy + 2 * kmax) * (kCostBx + 2 * kmax) +
-                  (size_t)(kCostBy + 2 * kmax) * kCostBx) * sizeof(float);
+    size_t pr = kCostBy + 2 * kmax, pcw = kCostBx + 2 * kmax;
+    size_t shm = (pr * pcw + pr * kCostBx + (pr + 1) * (pcw + 1)) * sizeof(float);
+    const bool w7 = kperp / 2 == 3 && kpar / 2 == 3;
     if (mode == CUPHU_COST_SMOOTH) {
-        if (shm > 48 * 1024)
-            cudaFuncSetAttribute(k_costs<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)shm);
-        k_costs<false><<<nblocks, 256, shm, s>>>(ph, corr, weights, nrow, ncol, kperp, kpar, k,
-                                                 costs, res, nbx0, nby0, nbx1);
+        if (w7) launch_costs_t<false, 3, 3>(nblocks, shm, s, ph, corr, weights, nrow, ncol, kperp, kpar, k, costs, res, nbx0, nby0, nbx1);
+        else launch_costs_t<false, 0, 0>(nblocks, shm, s, ph, corr, weights, nrow, ncol, kperp, kpar, k, costs, res, nbx0, nby0, nbx1);
     } else {
-        if (shm > 48 * 1024)
-            cudaFuncSetAttribute(k_costs<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)shm);
-        k_costs<true><<<nblocks, 256, shm, s>>>(ph, corr, weights, nrow, ncol, kperp, kpar, k,
-                                                costs, res, nbx0, nby0, nbx1);
+        if (w7) launch_costs_t<true, 3, 3>(nblocks, shm, s, ph, corr, weights, nrow, ncol, kperp, kpar, k, costs, res, nbx0, nby0, nbx1);
+        else launch_costs_t<true, 0, 0>(nblocks, shm, s, ph, corr, weights, nrow, ncol, kperp, kpar, k, costs, res, nbx0, nby0, nbx1);
     }
     return cuda_fail(cudaGetLastError(), "k_costs");
 }

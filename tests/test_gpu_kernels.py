@@ -213,3 +213,22 @@ def test_incrcost_matches_oracle_and_reference(torch_cuda):
     ex0 = check(lib().cuphu_incrcost_early_exit(dptr(dc), dptr(dz), c.shape[0], 200, 1,
                                                 dptr(dp), dptr(dn), dptr(ds)))
     assert bool(ex0) == O.incrcost(c, zero)[2]
+
+
+@pytest.mark.parametrize("nlooks", [1.0, 3.7, 20.0, 150.0])
+def test_cost_sigsq_screening_is_exact(torch_cuda, nlooks):
+    """The FP32 screening of the FP64 pow must never change a quantised
+    cost: dense random coherence over [0, 1] (plus exact 0 and 1), compared
+    with the reference kernels' pure-FP64 arithmetic on 2 M arcs."""
+    if O.ref_lib() is None:
+        pytest.skip("reference kernels not built")
+    rng = np.random.default_rng(int(nlooks * 10))
+    nr, nc = 1000, 1000
+    g = rng.random((nr, nc), dtype=np.float32)
+    g[::97, ::89] = 0.0
+    g[::83, ::71] = 1.0
+    ph = (rng.random((nr, nc)) * 2 * np.pi).astype(np.float32)
+    for mode in (0, 1):
+        got = gpu_costs(torch_cuda, ph, g, nlooks, mode)
+        ref, _ = O.ref_build_costs(ph, g, nlooks, mode=mode)
+        assert np.array_equal(got, ref), f"{np.sum(np.any(got != ref, axis=1))} arcs differ"
