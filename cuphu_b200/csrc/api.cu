@@ -291,6 +291,7 @@ static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpt
         P.wd = b.take<float>(np);
         P.wr = b.take<float>(np);
         P.x = b.take<double>(np);
+        P.dx = jo.fp64 ? nullptr : b.take<float>(np);
         P.r = b.take<char>(np * vs);
         P.p0 = b.take<char>(np * vs);
         P.p1 = b.take<char>(np * vs);

@@ -259,10 +259,16 @@ __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, b
         zv[j] = (V)z;
         if (write_diag) dv[j] = ds;
     }
-    st4(rr + prow + q.c0, rv);
+    if (sizeof(V) == 8) st4(rr + prow + q.c0, rv);
     st4((V *)P.z + T.pix + prow + q.c0, zv);
     if (write_diag) st4(dg + prow + q.c0, dv);
-    if (zero_x) st4(x + prow + q.c0, xv);
+    if (zero_x) {
+        st4(x + prow + q.c0, xv);
+        if (P.dx) {
+            const float zero[4] = {0.f, 0.f, 0.f, 0.f};
+            st4(P.dx + T.pix + prow + q.c0, zero);
+        }
+    }
     return acc;
 }
 
@@ -281,6 +287,7 @@ constexpr int kWrW = kItemBx + 4;         /* right-arc box incl. the left neighb
 struct SolveMaps {
     CUtensorMap zA, p0A, p1A, wdA, wrA;        /* stencil pass boxes */
     CUtensorMap xB, p0B, p1B, qB, rB, dB;      /* update pass boxes  */
+    CUtensorMap zB;                            /* mixed: z in place of r, dx in xB */
 };
 
 __host__ __device__ constexpr size_t al128(size_t b) { return (b + 127) & ~(size_t)127; }
@@ -293,11 +300,14 @@ template <typename V> struct StageA {
     static constexpr uint32_t kTx = (uint32_t)(2 * (kItemBy + 2) * kSegW * sizeof(V) +
                                                (kItemBy + 1) * kItemBx * 4 + kItemBy * kWrW * 4);
 };
+/* update-pass stage: FP64 mode x, p, q, r, diag; mixed mode dx (FP32) in the
+ * x slot, p, q, z (r = z diag is not stored) and diag */
 template <typename V> struct StageB {
     static constexpr size_t kX = (size_t)kItemBy * kItemBx * sizeof(double);
     static constexpr size_t kV = (size_t)kItemBy * kItemBx * sizeof(V);
     static constexpr size_t kBytes = kX + 4 * kV;
-    static constexpr uint32_t kTxFull = (uint32_t)(kX + 4 * kV);
+    static constexpr uint32_t kTxFull =
+        (uint32_t)((sizeof(V) == 4 ? (size_t)kItemBy * kItemBx * 4 : kX) + 4 * kV);
     static constexpr uint32_t kTxX = (uint32_t)(kX + kV);
 };
 #ifndef CUPHU_SOLVE_STAGES_F32
@@ -529,7 +539,7 @@ __device__ __forceinline__ void issue_b(const TileDesc &T, int li, const SolveMa
     tma_load_2d(PB, pnew_sel ? &M.p1B : &M.p0B, c0b, y, bar);
     if (update_r) {
         tma_load_2d(QB, &M.qB, c0b, y, bar);
-        tma_load_2d(RB, &M.rB, c0b, y, bar);
+        tma_load_2d(RB, sizeof(V) == 4 ? &M.zB : &M.rB, c0b, y, bar);
         tma_load_2d(DB, &M.dB, c0b, y, bar);
     }
 }
@@ -539,7 +549,6 @@ __device__ double compute_b(const TileDesc &T, int li, const SolverPlanes &P, do
                             bool update_r, const char *stage)
 {
     const int r0b = (li / T.nbx) * kItemBy, c0b = (li % T.nbx) * kItemBx;
-    const double *X = (const double *)stage;
     const V *PB = (const V *)(stage + StageB<V>::kX);
     const V *QB = PB + kItemBy * kItemBx;
     const V *RB = QB + kItemBy * kItemBx;
@@ -548,29 +557,45 @@ __device__ double compute_b(const TileDesc &T, int li, const SolverPlanes &P, do
     const int r = r0b + ty, c0 = c0b + tx * kItemVx;
     if (r >= T.nr || c0 >= T.nc) return 0.0;
     const int s0 = ty * kItemBx + tx * kItemVx;
-    double xv[4];
-    V pv[4], qv[4], rv[4] = {(V)0, (V)0, (V)0, (V)0}, dv[4], zv[4] = {(V)0, (V)0, (V)0, (V)0};
-    sld4(X + s0, xv);
-    sld4(PB + s0, pv);
-    if (update_r) {
-        sld4(QB + s0, qv);
-        sld4(RB + s0, rv);
-        sld4(DB + s0, dv);
-    }
-    const float alphaf = (float)alpha;
+    const size_t o = T.pix + (size_t)r * T.pitch + c0;
     double acc = 0.0;
+    if constexpr (sizeof(V) == 4) {
+        /* mixed: dx += alpha p (FP32), r = z diag, r -= alpha q, z = r / diag */
+        const float *DXB = (const float *)stage;
+        float dxv[4], pv[4], qv[4], zv[4], dv[4];
+        sld4(DXB + s0, dxv);
+        sld4((const float *)PB + s0, pv);
+        sld4((const float *)QB + s0, qv);
+        sld4((const float *)RB + s0, zv);
+        sld4((const float *)DB + s0, dv);
+        const float alphaf = (float)alpha;
 #pragma unroll
-    for (int j = 0; j < kItemVx; ++j) {
-        if (c0 + j >= T.nc) continue;
-        xv[j] = __fma_rn(alpha, (double)pv[j], xv[j]);
+        for (int j = 0; j < kItemVx; ++j) {
+            if (c0 + j >= T.nc) continue;
+            dxv[j] = __fmaf_rn(alphaf, pv[j], dxv[j]);
+            float rn = __fmaf_rn(-alphaf, qv[j], __fmul_rn(zv[j], dv[j]));
+            float z = __fdiv_rn(rn, dv[j]);
+            zv[j] = z;
+            acc = __fma_rn((double)rn, (double)z, acc);
+        }
+        st4(P.dx + o, dxv);
+        st4((float *)P.z + o, zv);
+    } else {
+        const double *X = (const double *)stage;
+        double xv[4];
+        V pv[4], qv[4], rv[4] = {(V)0, (V)0, (V)0, (V)0}, dv[4], zv[4] = {(V)0, (V)0, (V)0, (V)0};
+        sld4(X + s0, xv);
+        sld4(PB + s0, pv);
         if (update_r) {
-            if (sizeof(V) == 4) {
-                float rn = __fmaf_rn(-alphaf, (float)qv[j], (float)rv[j]);
-                float z = __fdiv_rn(rn, (float)dv[j]);
-                rv[j] = (V)rn;
-                zv[j] = (V)z;
-                acc = __fma_rn((double)rn, (double)z, acc);
-            } else {
+            sld4(QB + s0, qv);
+            sld4(RB + s0, rv);
+            sld4(DB + s0, dv);
+        }
+#pragma unroll
+        for (int j = 0; j < kItemVx; ++j) {
+            if (c0 + j >= T.nc) continue;
+            xv[j] = __fma_rn(alpha, (double)pv[j], xv[j]);
+            if (update_r) {
                 V rn = (V)__fma_rn(-alpha, (double)qv[j], (double)rv[j]);
                 rv[j] = rn;
                 double z = (double)rn / (double)dv[j];
@@ -578,14 +603,44 @@ __device__ double compute_b(const TileDesc &T, int li, const SolverPlanes &P, do
                 acc = __fma_rn((double)rn, z, acc);
             }
         }
-    }
-    size_t o = T.pix + (size_t)r * T.pitch + c0;
-    st4(P.x + o, xv);
-    if (update_r) {
-        st4((V *)P.r + o, rv);
-        st4((V *)P.z + o, zv);
+        st4(P.x + o, xv);
+        if (update_r) {
+            st4((V *)P.r + o, rv);
+            st4((V *)P.z + o, zv);
+        }
     }
     return acc;
+}
+
+template <typename V> __device__ __forceinline__ const V *pnew_last(V *const *pb, int it)
+{
+    return pb[(it + 1) & 1];
+}
+
+/* mixed precision: fold the FP32 increment into the FP64 solution, optionally
+ * applying this iteration's update first (x = x + (dx + alpha p), dx = 0) */
+template <typename V>
+__device__ void phase_fold(const TileDesc &T, int li, const SolverPlanes &P, const V *pnew_all,
+                           bool with_update, double alpha)
+{
+    ItemXY q = item_xy(T, li);
+    if (q.r >= T.nr || q.c0 >= T.nc) return;
+    const size_t o = T.pix + (size_t)q.r * T.pitch + q.c0;
+    float dxv[4], pv[4];
+    double xv[4];
+    ld4(P.dx + o, dxv);
+    ld4(P.x + o, xv);
+    if (with_update) ld4((const float *)pnew_all + o, pv);
+    const float alphaf = (float)alpha;
+#pragma unroll
+    for (int j = 0; j < kItemVx; ++j) {
+        if (q.c0 + j >= T.nc) continue;
+        float d = with_update ? __fmaf_rn(alphaf, pv[j], dxv[j]) : dxv[j];
+        xv[j] = xv[j] + (double)d;
+    }
+    const float zero[4] = {0.f, 0.f, 0.f, 0.f};
+    st4(P.x + o, xv);
+    st4(P.dx + o, zero);
 }
 
 /* ── IRLS reweight (A13): w = w0 / sqrt(e^2 + delta^2) ───────────────────── */
@@ -1015,9 +1070,22 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
                 }
             }
             __syncthreads();
-            run_pass<1, V>(sc, tiles, stB, ntiles, P, M, (it + 1) & 1, pnew, !repl, pbuf[pc & 1],
-                           sw, Pn, dsm, bars, parity, ctl, timeout_ns);
-            if (!repl) ++pc;
+            if (!repl) {
+                run_pass<1, V>(sc, tiles, stB, ntiles, P, M, (it + 1) & 1, pnew, true, pbuf[pc & 1],
+                               sw, Pn, dsm, bars, parity, ctl, timeout_ns);
+                ++pc;
+            } else {
+                /* fold this iteration's update into the FP64 solution; the
+                 * true residual follows once every neighbour has folded */
+                for (int t = sc.t0; t <= sc.t1; ++t) {
+                    const TileDesc &T = stile(sc, tiles, t);
+                    if (sc.pre[t + 1] == sc.pre[t] || !sactive(sc, stB, t)) continue;
+                    int a, b;
+                    slice_items(sc, T, t, a, b);
+                    double alpha = salpha(sc, stB, t);
+                    for (int li = a; li < b; ++li) phase_fold<V>(T, li, P, pnew, true, alpha);
+                }
+            }
             if (!grid_sync(ctl, timeout_ns)) return;
             if (repl) {
                 setup_slice(sc, tiles, stB, ntiles, sw);
@@ -1034,6 +1102,17 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
                 if (!grid_sync(ctl, timeout_ns)) return;
             }
             ++it;
+        }
+        if (mixed) {
+            /* fold the FP32 increments of the pass into the FP64 solution */
+            setup_slice(sc, tiles, nullptr, ntiles, sw);
+            for (int t = sc.t0; t <= sc.t1; ++t) {
+                const TileDesc &T = stile(sc, tiles, t);
+                int a, b;
+                slice_items(sc, T, t, a, b);
+                for (int li = a; li < b; ++li) phase_fold<V>(T, li, P, pnew_last(pb, it), false, 0.0);
+            }
+            if (!grid_sync(ctl, timeout_ns)) return;
         }
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             if (sp.pass_iters) sp.pass_iters[outer] = it;
@@ -1106,11 +1185,13 @@ static int make_maps(SolveMaps &M, const SolverPlanes &P, int pitch, int rows)
     rc |= make_map(M.p1A, P.p1, v, pitch, rows, kSegW, kItemBy + 2);
     rc |= make_map(M.wdA, P.wd, 4, pitch, rows, kItemBx, kItemBy + 1);
     rc |= make_map(M.wrA, P.wr, 4, pitch, rows, kWrW, kItemBy);
-    rc |= make_map(M.xB, P.x, 8, pitch, rows, kItemBx, kItemBy);
+    if (v == 4) rc |= make_map(M.xB, P.dx, 4, pitch, rows, kItemBx, kItemBy);
+    else rc |= make_map(M.xB, P.x, 8, pitch, rows, kItemBx, kItemBy);
+    rc |= make_map(M.zB, P.z, v, pitch, rows, kItemBx, kItemBy);
     rc |= make_map(M.p0B, P.p0, v, pitch, rows, kItemBx, kItemBy);
     rc |= make_map(M.p1B, P.p1, v, pitch, rows, kItemBx, kItemBy);
     rc |= make_map(M.qB, P.q, v, pitch, rows, kItemBx, kItemBy);
-    rc |= make_map(M.rB, P.r, v, pitch, rows, kItemBx, kItemBy);
+    rc |= make_map(M.rB, v == 8 ? P.r : P.z, v, pitch, rows, kItemBx, kItemBy);
     rc |= make_map(M.dB, P.diag, v, pitch, rows, kItemBx, kItemBy);
     return rc ? CUPHU_ERR_CUDA : 0;
 }
