@@ -119,6 +119,7 @@ SIGNATURES = {
     "cuphu_laplace_solve_device": (_I, [VP, _I, VP, _I, _I, P(CuPhuSolveOptions), VP, VP, VP,
                                         P(CuPhuSolveStats), VP]),
     "cuphu_integrate_phase_gpu": (_I, [VP, VP, VP, _I, _I, _I, VP]),
+    "cuphu_integrate_phase_noalloc": (_I, [VP, VP, VP, _I, _I, VP, VP]),
     "cuphu_conncomp_gpu": (_I, [VP, VP, VP, _I, _I, VP, VP, P(CuPhuParams), _I, VP]),
     "cuphu_conncomp_ex": (_I, [VP, VP, VP, _I, _I, C.c_float, _D, _L, _I, VP]),
     "cuphu_incrcost_early_exit": (_I, [VP, VP, _I, _L, _I, VP, VP, VP]),

@@ -262,6 +262,24 @@ int cuphu_integrate_phase_gpu(const float *wrapped_phase, const short *hflows,
                               const short *vflows, int nrow, int ncol, int gpu_id,
                               float *unw_out);
 
+/* ── integration without device allocation.  No counterpart in the
+ *    reference.
+ * Same result as cuphu_integrate_phase_gpu, for callers that cannot
+ * allocate device memory (a host framework whose caching allocator holds
+ * the device's memory, a real-time processor that forbids allocation after
+ * start-up).  Device pointers; enqueued on `stream` of the current device,
+ * no synchronisation.  The per-row scratch comes from a fixed array inside
+ * the library (CUPHU_NOALLOC_MAX_ROWS floats, held by every GPU that loads
+ * the library until exit), so nrow above CUPHU_NOALLOC_MAX_ROWS returns
+ * CUPHU_ERR_INVALID.  The first call on a device looks up the array's
+ * device address: make it before any stream capture.  All calls on a
+ * device share the array, so calls that overlap on the GPU race; order
+ * them on one stream or with events. */
+#define CUPHU_NOALLOC_MAX_ROWS 65536
+int cuphu_integrate_phase_noalloc(const float *wrapped_phase, const short *hflows,
+                                  const short *vflows, int nrow, int ncol, float *unw_out,
+                                  void *stream);
+
 /* ── connected components (ref cuphu.h:275-289, cuphu_conncomp.cu:290-428) */
 int cuphu_conncomp_gpu(const float *unw, const float *corr, const unsigned char *mask,
                        int nrow, int ncol, const short *poscost, const short *negcost,
