@@ -41,6 +41,11 @@ FALLBACK_HBM = 6650.0
 METRIC = "Mpix/s unwrapped at 8192^2 (mixed-precision Laplace PCG)"
 
 
+# measured k_solve DRAM bytes (mixed precision), see the roofline block
+TRAFFIC_PER_PX_ITER = 50.1
+TRAFFIC_PER_PASS_PX = 71.0
+
+
 def hbm_peak():
     try:
         with open(PEAKS) as f:
@@ -262,8 +267,14 @@ def run_ours(args, rank, world, local_rank):
     bpi = 36 if prec == 0 else 64
     alg_bytes = px_iters * bpi + (opts.n_irls + 1) * tile_px * 38
     achieved = alg_bytes / (st.solve_ms * 1e-3) / 1e9
+    # DRAM traffic per launch, scaled from ncu captures of the 4096^2 case
+    # (dram__bytes_read.sum + dram__bytes_write.sum at 20 and 40 iterations):
+    # the marginal bytes per active-tile pixel-iteration plus the fixed bytes
+    # per tile pixel of each IRLS pass (assemble/INIT and final)
+    traffic = (px_iters * TRAFFIC_PER_PX_ITER + (opts.n_irls + 1) * tile_px * TRAFFIC_PER_PASS_PX
+               if prec == 0 else None)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                 "kernel": "k_solve", "solve_ms": st.solve_ms, "pcg_iterations": st.total_iters,
                 "px_iterations": st.px_iters, "tile_px": tile_px,
                 "bytes_per_px_iter": bpi}

@@ -316,7 +316,8 @@ static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpt
         d_sout = b.take<SceneOut>(nsc);
         d_k = b.take<CostConsts>(nsc);
         d_st = b.take<TileState>(2 * (size_t)ntiles);
-        d_part = b.take<double>(2 * (size_t)pl.nitems);
+        /* item partials x2, published tile totals x2, tile item tickets */
+        d_part = b.take<double>(2 * (size_t)pl.nitems + 3 * (size_t)ntiles);
         d_ctl = b.take<SolverCtl>(1);
         d_deltas = b.take<float>(o.n_irls + 1);
         d_pass = b.take<int>(o.n_irls + 1);
@@ -399,6 +400,8 @@ static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpt
                                    cudaMemcpyHostToDevice, s));
     CUPHU_TRY_CUDA(cudaMemsetAsync(d_st, 0, 2 * ntiles * sizeof(TileState), s));
     CUPHU_TRY_CUDA(cudaMemsetAsync(d_ctl, 0, sizeof(SolverCtl), s));
+    CUPHU_TRY_CUDA(cudaMemsetAsync(d_part + 2 * (size_t)pl.nitems + 2 * (size_t)ntiles, 0,
+                                   (size_t)ntiles * sizeof(double), s));
 
     for (int i = 0; i < nsc; ++i) {
         if (S[i].ph_in) continue;

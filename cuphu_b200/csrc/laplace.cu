@@ -98,9 +98,11 @@ __device__ __forceinline__ void store_partial(double acc, double *part, int item
     if (threadIdx.x == 0) part[item] = bs;
 }
 
-/* block tree without the leading barrier, for item loops that already
- * separate consecutive uses of sw; returns after the barrier that follows
- * the warp sums, so every thread has finished the caller's work on the item */
+/* block tree without the leading barrier, for item loops: consecutive items
+ * pass alternating halves of the scratch (sw, sw + 8), so a warp that runs
+ * ahead into the next item never overwrites warp sums that warp 0 has not
+ * read; returns after the barrier that follows the warp sums, so every thread
+ * has finished the caller's work on the item */
 __device__ __forceinline__ double block_sum_item(double v, double *sw)
 {
     for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
@@ -112,6 +114,33 @@ __device__ __forceinline__ double block_sum_item(double v, double *sw)
         for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
     }
     return v;
+}
+
+/* A block has written the partials of its items [a, b) of tile t for this
+ * phase (thread 0 writes every partial of a block).  The block whose items
+ * complete the tile's count computes the canonical tile total once and
+ * publishes it in tot[t]; the other blocks move on.  The total is the same
+ * whichever block computes it, because tile_reduce fixes the order.  Readers
+ * pick it up after the next grid barrier. */
+__device__ void seg_done(const TileDesc &T, int t, int nseg, const double *part, double *tot,
+                         unsigned *cnt, double *sw, double *s_bcast, int *s_flag)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        unsigned prev = atomicAdd(&cnt[t], (unsigned)nseg);
+        int last = prev + (unsigned)nseg == (unsigned)T.nitems;
+        if (last) __threadfence();
+        *s_flag = last;
+    }
+    __syncthreads();
+    if (*s_flag) {
+        double v = tile_reduce(T, part, sw, s_bcast);
+        if (threadIdx.x == 0) {
+            tot[t] = v;
+            cnt[t] = 0u;
+        }
+    }
 }
 
 __device__ __forceinline__ unsigned long long globaltimer()
@@ -296,18 +325,20 @@ template <typename V> struct StageA {
     static constexpr size_t kVec = al128((size_t)(kItemBy + 2) * kSegW * sizeof(V));
     static constexpr size_t kWd = al128((size_t)(kItemBy + 1) * kItemBx * sizeof(float));
     static constexpr size_t kWr = al128((size_t)kItemBy * kWrW * sizeof(float));
-    static constexpr size_t kBytes = 2 * kVec + kWd + kWr;
+    /* mixed mode: the item's FP32 increment dx, which takes the previous
+     * iteration's deferred dx += alpha p_old */
+    static constexpr size_t kDx = sizeof(V) == 4 ? (size_t)kItemBy * kItemBx * 4 : 0;
+    static constexpr size_t kBytes = 2 * kVec + kWd + kWr + kDx;
     static constexpr uint32_t kTx = (uint32_t)(2 * (kItemBy + 2) * kSegW * sizeof(V) +
                                                (kItemBy + 1) * kItemBx * 4 + kItemBy * kWrW * 4);
 };
-/* update-pass stage: FP64 mode x, p, q, r, diag; mixed mode dx (FP32) in the
- * x slot, p, q, z (r = z diag is not stored) and diag */
+/* update-pass stage: FP64 mode x, p, q, r, diag; mixed mode q, z (r = z diag
+ * is not stored) and diag, back to back */
 template <typename V> struct StageB {
     static constexpr size_t kX = (size_t)kItemBy * kItemBx * sizeof(double);
     static constexpr size_t kV = (size_t)kItemBy * kItemBx * sizeof(V);
     static constexpr size_t kBytes = kX + 4 * kV;
-    static constexpr uint32_t kTxFull =
-        (uint32_t)((sizeof(V) == 4 ? (size_t)kItemBy * kItemBx * 4 : kX) + 4 * kV);
+    static constexpr uint32_t kTxFull = (uint32_t)(sizeof(V) == 4 ? 3 * kV : kX + 4 * kV);
     static constexpr uint32_t kTxX = (uint32_t)(kX + kV);
 };
 #ifndef CUPHU_SOLVE_STAGES_F32
@@ -321,6 +352,21 @@ template <typename V> __host__ __device__ constexpr size_t stage_bytes()
 {
     return al128(StageA<V>::kBytes > StageB<V>::kBytes ? StageA<V>::kBytes : StageB<V>::kBytes);
 }
+/* ring shape of a pass: the mixed update pass stages only q, z and diag
+ * (12 KB per item), so it runs four shallow stages in the memory of the two
+ * deep ones */
+constexpr size_t kStageBm = 3 * (size_t)kItemBy * kItemBx * 4;
+template <int KIND, typename V> __host__ __device__ constexpr int pass_stages()
+{
+    return (KIND == 1 && sizeof(V) == 4) ? 4 : n_stages<V>();
+}
+template <int KIND, typename V> __host__ __device__ constexpr size_t pass_stage_bytes()
+{
+    return (KIND == 1 && sizeof(V) == 4) ? kStageBm : stage_bytes<V>();
+}
+static_assert(pass_stages<1, float>() * pass_stage_bytes<1, float>() <=
+                  n_stages<float>() * stage_bytes<float>(),
+              "mixed update-pass ring exceeds the stage memory");
 /* p_new of an item with its halo ring, rows of kSegW elements laid out like
  * the staged boxes (column 0 <-> c0b - 4), so own columns start 16-byte
  * aligned at column 4 */
@@ -394,7 +440,7 @@ __device__ __forceinline__ void fence_async_global()
 
 template <typename V>
 __device__ __forceinline__ void issue_a(const TileDesc &T, int li, const SolveMaps &M, int pold_sel,
-                                        bool first, char *stage, uint64_t *bar)
+                                        bool first, bool upd, char *stage, uint64_t *bar)
 {
     const int r0b = (li / T.nbx) * kItemBy, c0b = (li % T.nbx) * kItemBx;
     const int y = T.row0 + r0b;
@@ -402,12 +448,15 @@ __device__ __forceinline__ void issue_a(const TileDesc &T, int li, const SolveMa
     char *PO = stage + StageA<V>::kVec;
     char *WD = PO + StageA<V>::kVec;
     char *WR = WD + StageA<V>::kWd;
+    char *DX = WR + StageA<V>::kWr;
     uint32_t tx = StageA<V>::kTx - (first ? (uint32_t)((kItemBy + 2) * kSegW * sizeof(V)) : 0u);
+    if (upd) tx += (uint32_t)StageA<V>::kDx;
     mbar_expect(bar, tx);
     tma_load_2d(Z, &M.zA, c0b - 4, y - 1, bar);
     if (!first) tma_load_2d(PO, pold_sel ? &M.p1A : &M.p0A, c0b - 4, y - 1, bar);
     tma_load_2d(WD, &M.wdA, c0b, y - 1, bar);
     tma_load_2d(WR, &M.wrA, c0b - 4, y, bar);
+    if (upd) tma_load_2d(DX, &M.xB, c0b, y, bar);
 }
 
 /* shared-memory vector access of 4 consecutive elements (16-byte aligned) */
@@ -435,10 +484,14 @@ __device__ __forceinline__ V pupdate(bool first, double beta, float betaf, V po,
 /* stencil pass on a staged item: p_new = z + beta p_old (own + halo ring),
  * q = A p_new, thread partial of p.q (FP64 accumulation).  FP64 mode: FP64
  * arithmetic in the oracle's operation order.  Mixed mode: FP32 arithmetic
- * (the SpMV and vector update), FP64 only for the dot. */
+ * (the SpMV and vector update), FP64 only for the dot; with upd it also
+ * applies the previous iteration's solution update dx += alpha_prev p_old,
+ * which the update pass leaves to this pass because p_old is staged here
+ * anyway. */
 template <typename V>
 __device__ double compute_a(const TileDesc &T, int li, const SolverPlanes &P, V *pnew_all,
-                            bool first, double beta, const char *stage, V *Pn)
+                            bool first, double beta, bool upd, double alpha_prev,
+                            const char *stage, V *Pn)
 {
     const int r0b = (li / T.nbx) * kItemBy, c0b = (li % T.nbx) * kItemBx;
     const V *Z = (const V *)stage;
@@ -460,6 +513,19 @@ __device__ double compute_a(const TileDesc &T, int li, const SolverPlanes &P, V 
 #pragma unroll
         for (int j = 0; j < kItemVx; ++j)
             if (c0 + j < nc) pn[j] = pupdate<V>(first, beta, betaf, pv[j], zv[j]);
+        if constexpr (sizeof(V) == 4) {
+            if (upd) {
+                const float *DX = (const float *)(stage + 2 * StageA<V>::kVec + StageA<V>::kWd +
+                                                  StageA<V>::kWr);
+                float dxv[4];
+                sld4(DX + ty * kItemBx + tx * kItemVx, dxv);
+                const float af = (float)alpha_prev;
+#pragma unroll
+                for (int j = 0; j < kItemVx; ++j)
+                    if (c0 + j < nc) dxv[j] = __fmaf_rn(af, (float)pv[j], dxv[j]);
+                st4(P.dx + T.pix + (size_t)r * T.pitch + c0, dxv);
+            }
+        }
     }
 #pragma unroll
     for (int j = 0; j < kItemVx; ++j) Pn[so + j] = pn[j];
@@ -529,6 +595,15 @@ __device__ __forceinline__ void issue_b(const TileDesc &T, int li, const SolveMa
 {
     const int r0b = (li / T.nbx) * kItemBy, c0b = (li % T.nbx) * kItemBx;
     const int y = T.row0 + r0b;
+    if (sizeof(V) == 4) {
+        /* mixed: q, z, diag back to back */
+        char *QB = stage;
+        mbar_expect(bar, StageB<V>::kTxFull);
+        tma_load_2d(QB, &M.qB, c0b, y, bar);
+        tma_load_2d(QB + StageB<V>::kV, &M.zB, c0b, y, bar);
+        tma_load_2d(QB + 2 * StageB<V>::kV, &M.dB, c0b, y, bar);
+        return;
+    }
     char *X = stage;
     char *PB = X + StageB<V>::kX;
     char *QB = PB + StageB<V>::kV;
@@ -539,7 +614,7 @@ __device__ __forceinline__ void issue_b(const TileDesc &T, int li, const SolveMa
     tma_load_2d(PB, pnew_sel ? &M.p1B : &M.p0B, c0b, y, bar);
     if (update_r) {
         tma_load_2d(QB, &M.qB, c0b, y, bar);
-        tma_load_2d(RB, sizeof(V) == 4 ? &M.zB : &M.rB, c0b, y, bar);
+        tma_load_2d(RB, &M.rB, c0b, y, bar);
         tma_load_2d(DB, &M.dB, c0b, y, bar);
     }
 }
@@ -560,25 +635,22 @@ __device__ double compute_b(const TileDesc &T, int li, const SolverPlanes &P, do
     const size_t o = T.pix + (size_t)r * T.pitch + c0;
     double acc = 0.0;
     if constexpr (sizeof(V) == 4) {
-        /* mixed: dx += alpha p (FP32), r = z diag, r -= alpha q, z = r / diag */
-        const float *DXB = (const float *)stage;
-        float dxv[4], pv[4], qv[4], zv[4], dv[4];
-        sld4(DXB + s0, dxv);
-        sld4((const float *)PB + s0, pv);
-        sld4((const float *)QB + s0, qv);
-        sld4((const float *)RB + s0, zv);
-        sld4((const float *)DB + s0, dv);
+        /* mixed: r = z diag, r -= alpha q, z = r / diag (the solution update
+         * dx += alpha p is deferred to the next stencil pass or fold) */
+        const float *QM = (const float *)stage;
+        float qv[4], zv[4], dv[4];
+        sld4(QM + s0, qv);
+        sld4(QM + kItemBy * kItemBx + s0, zv);
+        sld4(QM + 2 * kItemBy * kItemBx + s0, dv);
         const float alphaf = (float)alpha;
 #pragma unroll
         for (int j = 0; j < kItemVx; ++j) {
             if (c0 + j >= T.nc) continue;
-            dxv[j] = __fmaf_rn(alphaf, pv[j], dxv[j]);
             float rn = __fmaf_rn(-alphaf, qv[j], __fmul_rn(zv[j], dv[j]));
             float z = __fdiv_rn(rn, dv[j]);
             zv[j] = z;
             acc = __fma_rn((double)rn, (double)z, acc);
         }
-        st4(P.dx + o, dxv);
         st4((float *)P.z + o, zv);
     } else {
         const double *X = (const double *)stage;
@@ -610,11 +682,6 @@ __device__ double compute_b(const TileDesc &T, int li, const SolverPlanes &P, do
         }
     }
     return acc;
-}
-
-template <typename V> __device__ __forceinline__ const V *pnew_last(V *const *pb, int it)
-{
-    return pb[(it + 1) & 1];
 }
 
 /* mixed precision: fold the FP32 increment into the FP64 solution, optionally
@@ -754,6 +821,15 @@ __device__ __forceinline__ double salpha(const SliceCtl &sc, const TileState *st
     int k = t - sc.t0;
     return (k >= 0 && k < sc.ncached) ? sc.alpha[k] : __ldcg(&st[t].alpha);
 }
+/* Every block touching a tile derives the same scalars; only the tile's owner
+ * publishes them (hundreds of blocks storing one line serialise in L2 when a
+ * single tile is left).  A block reads its own copy from the cache, or, for a
+ * tile beyond the cache, from the global state it then writes itself. */
+__device__ __forceinline__ bool scached(const SliceCtl &sc, int t)
+{
+    int k = t - sc.t0;
+    return k >= 0 && k < sc.ncached;
+}
 __device__ __forceinline__ void sput(SliceCtl &sc, int t, const TileState &S)
 {
     int k = t - sc.t0;
@@ -868,6 +944,14 @@ __device__ __forceinline__ Cursor cursor_active(Cursor c, const SliceCtl &sc, co
     return c;
 }
 
+/* mixed mode: the stencil pass of an iteration applies the previous
+ * iteration's deferred solution update unless there is none (first
+ * iteration, or alpha_prev zeroed because a fold already applied it) */
+template <typename V> __device__ __forceinline__ bool defer_upd(bool first, double alpha_prev)
+{
+    return sizeof(V) == 4 && !first && alpha_prev != 0.0;
+}
+
 /* run a staged pass over this block's slice.  KIND 0: the stencil pass,
  * KIND 1: the update pass.  NS items are in flight; the stage of item k is
  * refilled with item k+NS right after the barrier of item k's reduction,
@@ -875,11 +959,13 @@ __device__ __forceinline__ Cursor cursor_active(Cursor c, const SliceCtl &sc, co
 template <int KIND, typename V>
 __device__ void run_pass(const SliceCtl &sc, const TileDesc *gt, const TileState *st, int ntiles,
                          const SolverPlanes &P, const SolveMaps &M, int psel, V *pvec, bool flag,
-                         double *part, double *sw, V *Pn, char *stages, uint64_t *bars,
-                         uint32_t &parity, SolverCtl *ctl, long long timeout_ns)
+                         double *part, double *tot, unsigned *cnt, double *sw, double *s_bcast,
+                         int *s_flag, V *Pn, char *stages, uint64_t *bars, uint32_t &parity,
+                         SolverCtl *ctl, long long timeout_ns)
 {
-    constexpr int NS = n_stages<V>();
-    constexpr size_t SB = stage_bytes<V>();
+    constexpr int NS = pass_stages<KIND, V>();
+    constexpr size_t SB = pass_stage_bytes<KIND, V>();
+    const bool red = KIND == 0 || flag;
     if (sc.s0 >= sc.s1) return;
     Cursor ci = cursor_active(Cursor{sc.s0, sc.t0}, sc, gt, st, ntiles);
     if (ci.p >= sc.s1) return;
@@ -892,7 +978,9 @@ __device__ void run_pass(const SliceCtl &sc, const TileDesc *gt, const TileState
         if (threadIdx.x == 0) {
             const TileDesc &T = stile(sc, gt, ci.t);
             int li = ci.p - sc.pre[ci.t];
-            if (KIND == 0) issue_a<V>(T, li, M, psel, flag, stages + k * SB, bars + k);
+            if (KIND == 0)
+                issue_a<V>(T, li, M, psel, flag, defer_upd<V>(flag, salpha(sc, st, ci.t)),
+                           stages + k * SB, bars + k);
             else issue_b<V>(T, li, M, psel, flag, stages + k * SB, bars + k);
         }
         ci = cursor_active(Cursor{ci.p + 1, ci.t}, sc, gt, st, ntiles);
@@ -906,23 +994,33 @@ __device__ void run_pass(const SliceCtl &sc, const TileDesc *gt, const TileState
         const TileDesc &T = stile(sc, gt, cc.t);
         int li = cc.p - sc.pre[cc.t];
         double acc;
-        if (KIND == 0)
-            acc = compute_a<V>(T, li, P, pvec, flag, sbeta(sc, st, cc.t), stages + s * SB, Pn);
-        else
+        if (KIND == 0) {
+            const double ap = salpha(sc, st, cc.t);
+            acc = compute_a<V>(T, li, P, pvec, flag, sbeta(sc, st, cc.t), defer_upd<V>(flag, ap),
+                               ap, stages + s * SB, Pn);
+        } else
             acc = compute_b<V>(T, li, P, salpha(sc, st, cc.t), flag, stages + s * SB);
-        double bs = block_sum_item(acc, sw);   /* contains the item barrier */
+        double bs = block_sum_item(acc, sw + 8 * (done & 1));   /* contains the item barrier */
         if (threadIdx.x == 0) {
-            if (KIND == 0 || flag) part[T.item0 + li] = bs;
+            if (red) part[T.item0 + li] = bs;
             if (ci.p < sc.s1) {
                 fence_async_smem();
                 const TileDesc &Tn = stile(sc, gt, ci.t);
                 int ln = ci.p - sc.pre[ci.t];
-                if (KIND == 0) issue_a<V>(Tn, ln, M, psel, flag, stages + s * SB, bars + s);
+                if (KIND == 0)
+                    issue_a<V>(Tn, ln, M, psel, flag, defer_upd<V>(flag, salpha(sc, st, ci.t)),
+                               stages + s * SB, bars + s);
                 else issue_b<V>(Tn, ln, M, psel, flag, stages + s * SB, bars + s);
             }
         }
         if (ci.p < sc.s1) ci = cursor_active(Cursor{ci.p + 1, ci.t}, sc, gt, st, ntiles);
-        cc = cursor_active(Cursor{cc.p + 1, cc.t}, sc, gt, st, ntiles);
+        Cursor nx = cursor_active(Cursor{cc.p + 1, cc.t}, sc, gt, st, ntiles);
+        if (red && (nx.p >= sc.s1 || nx.t != cc.t)) {
+            int a, b;
+            slice_items(sc, T, cc.t, a, b);
+            seg_done(T, cc.t, b - a, part, tot, cnt, sw, s_bcast, s_flag);
+        }
+        cc = nx;
     }
     __syncthreads();
 }
@@ -954,18 +1052,24 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
     extern __shared__ __align__(128) char dsm_raw[];
     __shared__ double sw[32];
     __shared__ double s_bcast;
+    __shared__ int s_flag;
     __shared__ __align__(8) uint64_t bars[4];
     __shared__ SliceCtl sc;
     constexpr int NS = n_stages<V>();
+    constexpr int NBAR = pass_stages<1, V>() > NS ? pass_stages<1, V>() : NS;
     char *dsm = (char *)(((uintptr_t)dsm_raw + 127) & ~(uintptr_t)127);
     const bool mixed = sizeof(V) == 4;
     V *pb[2] = {(V *)P.p0, (V *)P.p1};
+    /* per-item partials and published tile totals, both double-buffered by
+     * phase parity, and the per-tile item tickets */
     double *pbuf[2] = {part, part + nitems};
+    double *tbuf[2] = {part + 2 * (size_t)nitems, part + 2 * (size_t)nitems + ntiles};
+    unsigned *tick = reinterpret_cast<unsigned *>(part + 2 * (size_t)nitems + 2 * (size_t)ntiles);
     V *Pn = (V *)(dsm + NS * stage_bytes<V>());
     uint32_t parity = 0u;
     (void)item_tile;
     if (threadIdx.x == 0) {
-        for (int k = 0; k < NS; ++k) mbar_init(&bars[k]);
+        for (int k = 0; k < NBAR; ++k) mbar_init(&bars[k]);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -981,6 +1085,7 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
             for (int li = a; li < b; ++li)
                 store_partial(phase_init<V>(T, li, P, outer == 0, true), pbuf[pc & 1],
                               T.item0 + li, sw);
+            if (b > a) seg_done(T, t, b - a, pbuf[pc & 1], tbuf[pc & 1], tick, sw, &s_bcast, &s_flag);
         }
         ++pc;
         if (!grid_sync(ctl, timeout_ns)) return;
@@ -1005,7 +1110,7 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
                 const bool owner = sc.pre[t] >= sc.s0 && sc.pre[t] < sc.s1;
                 TileState S;
                 if (it == 0) {
-                    double tot = tile_reduce(T, pbuf[(pc - 1) & 1], sw, &s_bcast);
+                    double tot = __ldcg(tbuf[(pc - 1) & 1] + t);
                     S.rz = tot;
                     S.rz0 = tot;
                     S.thr = (double)sp.tol * (double)sp.tol * tot;
@@ -1016,7 +1121,10 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
                     if (owner && threadIdx.x == 0 && S.active) atomicAdd(&ctl->n_active, 1);
                 } else {
                     S = load_state(stB + t);
-                    double tot = tile_reduce(T, pbuf[(pc - 1) & 1], sw, &s_bcast);
+                    double tot = __ldcg(tbuf[(pc - 1) & 1] + t);
+                    /* a replacement iteration folded its update already */
+                    if (mixed && sp.replace_every > 0 && (it % sp.replace_every) == 0)
+                        S.alpha = 0.0;
                     S.iter += 1;
                     if (tot < S.thr || S.iter >= sp.max_iter) {
                         S.active = 0;
@@ -1031,13 +1139,14 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
                     }
                 }
                 if (threadIdx.x == 0) {
-                    stA[t] = S;
+                    if (owner || !scached(sc, t)) stA[t] = S;
                     sput(sc, t, S);
                 }
             }
             __syncthreads();
-            run_pass<0, V>(sc, tiles, stA, ntiles, P, M, it & 1, pnew, it == 0, pbuf[pc & 1], sw,
-                           Pn, dsm, bars, parity, ctl, timeout_ns);
+            run_pass<0, V>(sc, tiles, stA, ntiles, P, M, it & 1, pnew, it == 0, pbuf[pc & 1],
+                           tbuf[pc & 1], tick, sw, &s_bcast, &s_flag, Pn, dsm, bars, parity, ctl,
+                           timeout_ns);
             ++pc;
             if (!grid_sync(ctl, timeout_ns)) return;
             if (*(volatile int *)&ctl->snap <= 0) break;
@@ -1053,9 +1162,10 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
                 if (sc.pre[t + 1] == sc.pre[t]) continue;
                 const bool owner = sc.pre[t] >= sc.s0 && sc.pre[t] < sc.s1;
                 TileState S = load_state(stA + t);
-                double pq = tile_reduce(T, pbuf[(pc - 1) & 1], sw, &s_bcast);
+                double pq = __ldcg(tbuf[(pc - 1) & 1] + t);
                 if (pq <= 0.0) {
                     S.active = 0;
+                    S.alpha = 0.0;
                     if (owner && threadIdx.x == 0) {
                         atomicSub(&ctl->n_active, 1);
                         atomicAdd(&ctl->px_iters, (unsigned long long)S.iter *
@@ -1065,14 +1175,15 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
                     S.alpha = S.rz / pq;
                 }
                 if (threadIdx.x == 0) {
-                    stB[t] = S;
+                    if (owner || !scached(sc, t)) stB[t] = S;
                     sput(sc, t, S);
                 }
             }
             __syncthreads();
             if (!repl) {
                 run_pass<1, V>(sc, tiles, stB, ntiles, P, M, (it + 1) & 1, pnew, true, pbuf[pc & 1],
-                               sw, Pn, dsm, bars, parity, ctl, timeout_ns);
+                               tbuf[pc & 1], tick, sw, &s_bcast, &s_flag, Pn, dsm, bars, parity,
+                               ctl, timeout_ns);
                 ++pc;
             } else {
                 /* fold this iteration's update into the FP64 solution; the
@@ -1097,6 +1208,9 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
                     for (int li = a; li < b; ++li)
                         store_partial(phase_init<V>(T, li, P, false, false), pbuf[pc & 1],
                                       T.item0 + li, sw);
+                    if (b > a)
+                        seg_done(T, t, b - a, pbuf[pc & 1], tbuf[pc & 1], tick, sw, &s_bcast,
+                                 &s_flag);
                 }
                 ++pc;
                 if (!grid_sync(ctl, timeout_ns)) return;
@@ -1104,13 +1218,22 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
             ++it;
         }
         if (mixed) {
-            /* fold the FP32 increments of the pass into the FP64 solution */
+            /* fold the FP32 increments of the pass into the FP64 solution,
+             * with each tile's deferred last update: a tile that stopped in
+             * an r.z reduction at iteration i (stA.iter = i, stB.iter = i-1)
+             * still owes alpha_{i-1} p_{i-1} (p in pb[i & 1]; alpha zeroed
+             * when a replacement fold applied it); one that stopped in a p.q
+             * reduction (stA.iter = stB.iter) owes nothing */
             setup_slice(sc, tiles, nullptr, ntiles, sw);
             for (int t = sc.t0; t <= sc.t1; ++t) {
                 const TileDesc &T = stile(sc, tiles, t);
                 int a, b;
                 slice_items(sc, T, t, a, b);
-                for (int li = a; li < b; ++li) phase_fold<V>(T, li, P, pnew_last(pb, it), false, 0.0);
+                if (a >= b) continue;
+                const int ia = __ldcg(&stA[t].iter), ib = __ldcg(&stB[t].iter);
+                const double ap = ia == ib ? 0.0 : __ldcg(&stA[t].alpha);
+                const V *pl = pb[ia & 1];
+                for (int li = a; li < b; ++li) phase_fold<V>(T, li, P, pl, ap != 0.0, ap);
             }
             if (!grid_sync(ctl, timeout_ns)) return;
         }
