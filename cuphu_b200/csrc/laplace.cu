@@ -1025,6 +1025,67 @@ __device__ void run_pass(const SliceCtl &sc, const TileDesc *gt, const TileState
     __syncthreads();
 }
 
+/* Mixed-precision update pass without shared-memory staging.  The pass is
+ * elementwise (r = z diag - alpha q, z = r / diag) plus the r.z dot, so the
+ * block sweeps its slice's pixel rows with 16-byte loads straight from HBM
+ * (one contiguous row span per plane at a time, not 256-byte item rows), and
+ * each thread accumulates r.z in FP64 over the whole tile segment: one block reduction
+ * per tile segment instead of one per item, no barrier per item.  The
+ * segment total goes into the partial slot of the segment's first item and
+ * the segment's other slots are zeroed, so the tile total is the canonical
+ * sum over the tile's partials as in the other phases (deterministic for a
+ * given grid; mixed mode does not follow the oracle's summation order). */
+__device__ void run_update_direct(const SliceCtl &sc, const TileDesc *gt, const TileState *st,
+                                  const SolverPlanes &P, double *part, double *tot,
+                                  unsigned *cnt, double *sw, double *s_bcast, int *s_flag)
+{
+    for (int t = sc.t0; t <= sc.t1; ++t) {
+        if (sc.pre[t + 1] == sc.pre[t] || !sactive(sc, st, t)) continue;
+        const TileDesc &T = stile(sc, gt, t);
+        int a, b;
+        slice_items(sc, T, t, a, b);
+        if (a >= b) continue;
+        const float alphaf = (float)salpha(sc, st, t);
+        const int nr = T.nr, nc = T.nc, nbx = T.nbx;
+        float *zp = (float *)P.z + T.pix;
+        const float *qp = (const float *)P.q + T.pix, *dp = (const float *)P.diag + T.pix;
+        double acc = 0.0;
+        /* the segment's items, band by band (16-row strips), each strip swept
+         * one pixel row at a time across the segment's columns of the band */
+        for (int band = a / nbx; band <= (b - 1) / nbx; ++band) {
+            const int i0 = max(a, band * nbx) - band * nbx, i1 = min(b, (band + 1) * nbx) - band * nbx;
+            const int clo = i0 * kItemBx, chi = min(i1 * kItemBx, nc);
+            const int rlo = band * kItemBy, rhi = min(rlo + kItemBy, nr);
+            for (int r = rlo; r < rhi; ++r) {
+                for (int c0 = clo + (int)threadIdx.x * kItemVx; c0 < chi; c0 += blockDim.x * kItemVx) {
+                    const size_t o = (size_t)r * T.pitch + c0;
+                    float4 qv = __ldcs(reinterpret_cast<const float4 *>(qp + o));
+                    float4 zv = __ldcg(reinterpret_cast<const float4 *>(zp + o));
+                    float4 dv = __ldcg(reinterpret_cast<const float4 *>(dp + o));
+                    const int n4 = min(chi - c0, kItemVx);
+                    float q4[4] = {qv.x, qv.y, qv.z, qv.w};
+                    float z4[4] = {zv.x, zv.y, zv.z, zv.w};
+                    float d4[4] = {dv.x, dv.y, dv.z, dv.w};
+#pragma unroll
+                    for (int j = 0; j < kItemVx; ++j) {
+                        if (j >= n4) continue;
+                        float rn = __fmaf_rn(-alphaf, q4[j], __fmul_rn(z4[j], d4[j]));
+                        float z = __fdiv_rn(rn, d4[j]);
+                        z4[j] = z;
+                        acc = __fma_rn((double)rn, (double)z, acc);
+                    }
+                    st4(zp + o, z4);
+                }
+            }
+        }
+        double v = block_sum(acc, sw);
+        if (threadIdx.x == 0) part[T.item0 + a] = v;
+        for (int li = a + 1 + (int)threadIdx.x; li < b; li += blockDim.x) part[T.item0 + li] = 0.0;
+        __threadfence();
+        seg_done(T, t, b - a, part, tot, cnt, sw, s_bcast, s_flag);
+    }
+}
+
 /* state written by other blocks before the last grid barrier: read from L2 */
 __device__ __forceinline__ TileState load_state(const TileState *p)
 {
@@ -1181,9 +1242,13 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
             }
             __syncthreads();
             if (!repl) {
-                run_pass<1, V>(sc, tiles, stB, ntiles, P, M, (it + 1) & 1, pnew, true, pbuf[pc & 1],
-                               tbuf[pc & 1], tick, sw, &s_bcast, &s_flag, Pn, dsm, bars, parity,
-                               ctl, timeout_ns);
+                if (mixed)
+                    run_update_direct(sc, tiles, stB, P, pbuf[pc & 1], tbuf[pc & 1], tick, sw,
+                                      &s_bcast, &s_flag);
+                else
+                    run_pass<1, V>(sc, tiles, stB, ntiles, P, M, (it + 1) & 1, pnew, true,
+                                   pbuf[pc & 1], tbuf[pc & 1], tick, sw, &s_bcast, &s_flag, Pn, dsm,
+                                   bars, parity, ctl, timeout_ns);
                 ++pc;
             } else {
                 /* fold this iteration's update into the FP64 solution; the
