@@ -79,6 +79,14 @@ struct CostConsts {
     double screen;    /* relative half-width of the screening interval */
     float screen_f, sig_f, corr_f, scale_f;   /* FP32 screening constants */
     int dzmax;        /* DEFO discontinuity shelf in short-cycle steps */
+    /* FP32 fast path of the default-window cost kernel (k_costs7); fast = 0
+     * when its error bounds do not hold for these parameters */
+    int fast;
+    float nsc_f;          /* nshortcycle (exact in float) */
+    float thr_lo, thr_hi; /* coherence threshold bracket, 2^-20 relative */
+    float a_f, c_f;       /* v = a_f b^rhopow + c_f (weight 1) */
+    float m_off;          /* offset rounding margin */
+    int s_rho0;           /* truncated sigsq of a zero-coherence arc, weight 1 */
 };
 
 CostConsts make_cost_consts(const CuPhuParams &p);

@@ -51,6 +51,30 @@ CostConsts make_cost_consts(const CuPhuParams &p)
     double dz = std::nearbyint(k.nsc * k.defomax);
     int dzi = (dz != dz) ? 0 : (dz >= 2147483647.0 ? 2147483647 : (dz <= -2147483648.0 ? (int)-2147483647 - 1 : (int)dz));
     k.dzmax = std::max(1, std::min(dzi, 32767));
+
+    /* FP32 fast path (k_costs7): every quantity it rounds is bracketed by a
+     * margin above its FP32 error bound; see arc_fast */
+    k.fast = 0;
+    k.nsc_f = (float)k.nsc;
+    k.thr_lo = std::nextafter((float)(k.thresh * (1.0 - std::ldexp(1.0, -20))), 0.0f);
+    k.thr_hi = std::nextafter((float)(k.thresh * (1.0 + std::ldexp(1.0, -20))), 3.0e38f);
+    k.a_f = (float)(k.sigsqrhoconst * k.nsc2 / k.costscale);
+    k.c_f = (float)(k.sigsqcorr * k.nsc2 / k.costscale);
+    k.m_off = (float)(std::fabs(k.nsc) * std::ldexp(1.0, -22) + std::ldexp(1.0, -30));
+    /* the reference's FP64 arithmetic at rho = 0 (pow(1, rhopow) = 1) */
+    double t0 = std::fma(k.sigsqrhoconst, 1.0, k.sigsqcorr);
+    t0 = t0 * k.nsc2;
+    t0 = t0 / (k.costscale * 1.0);
+    k.s_rho0 = (t0 >= 0.0 && t0 < 1.0e6) ? (int)t0 : -1;
+    const bool ok = k.nsc > 0.0 && k.nsc <= 4096.0 && (double)k.nsc_f == k.nsc &&
+                    std::isfinite(k.costscale) && k.costscale > 0.0 &&
+                    std::isfinite(k.sigsqrhoconst) && k.sigsqrhoconst >= 0.0 &&
+                    std::isfinite(k.sigsqcorr) && k.sigsqcorr >= 0.0 &&
+                    std::isfinite(k.rhopow) && k.rhopow > 0.0 && k.rhopow < 64.0 &&
+                    std::isfinite(k.thresh) && k.thresh > 0.0 && k.thresh < 1.0 &&
+                    std::isfinite(k.a_f) && std::isfinite(k.c_f) && k.s_rho0 >= 0 &&
+                    std::isfinite(k.nsc2);
+    k.fast = ok ? 1 : 0;
     return k;
 }
 
@@ -102,6 +126,36 @@ __device__ __forceinline__ float ex2_approx(float x)
     return y;
 }
 
+/* ── division by the path's two constants ─────────────────────────────────
+ * x / c correctly rounded for c = 2 pi (wrapped differences) and c = 7 (the
+ * default box-car length), with zc = RN(1/c): q0 = RN(x zc), r = x - q0 c
+ * (exact through the FMA), q = RN(q0 + r zc) -- the correction step of
+ * P. Markstein, "Computation of elementary functions on the IBM RISC
+ * System/6000 processor", IBM J. Res. Develop. 34(1), 1990.  An exhaustive
+ * comparison with IEEE division over every float of the ranges used
+ * (tests/test_const_division.py) finds it exact for 2^-104 <= |x| <= 6.6
+ * when c = 2 pi, and for every |x| <= 3.6 except -0 when c = 7.  Phase
+ * differences outside that range take the IEEE division; box-car sums are
+ * bounded by 3.5 and never -0 (they accumulate from +0). */
+constexpr float kRcpTwoPiRN = 0x1.45f306p-3f;   /* RN(1 / (float)2pi) */
+constexpr float kRcp7RN = 0x1.24924ap-3f;       /* RN(1 / 7) */
+
+__device__ __forceinline__ float div_2pi(float x)
+{
+    const float a = fabsf(x);
+    if (!(a >= 0x1p-104f && a <= 6.6f)) return __fdiv_rn(x, kTwoPiF);
+    const float q0 = __fmul_rn(x, kRcpTwoPiRN);
+    const float r = __fmaf_rn(-q0, kTwoPiF, x);
+    return __fmaf_rn(r, kRcpTwoPiRN, q0);
+}
+
+__device__ __forceinline__ float div_7(float x)
+{
+    const float q0 = __fmul_rn(x, kRcp7RN);
+    const float r = __fmaf_rn(-q0, 7.0f, x);
+    return __fmaf_rn(r, kRcp7RN, q0);
+}
+
 /* (int)sigsq_f of the reference (cuphu_cost.cu:109-117) for a coherence rho
  * already thresholded.  The FP64 pow dominates the kernel's cost, and only
  * the truncated value matters, so it is screened first with an FP32 pow
@@ -110,6 +164,14 @@ __device__ __forceinline__ float ex2_approx(float x)
  * contains no integer the truncated result is certain.  Everything else (intervals that straddle an integer,
  * bases outside (0,1], non-positive weights) takes the exact FP64 path, so
  * the result is bit-identical to the reference arithmetic. */
+/* the reference's FP64 arithmetic (cuphu_cost.cu:109-117); out of line, the
+ * screen above sends it about one arc in a hundred */
+__device__ __noinline__ int trunc_sigsq_exact(double b, short w, const CostConsts &k)
+{
+    double sigsqrho = __dmul_rn(__fma_rn(k.sigsqrhoconst, pow(b, k.rhopow), k.sigsqcorr), k.nsc2);
+    return (int)(sigsqrho / (k.costscale * (double)w));
+}
+
 __device__ __forceinline__ int trunc_sigsq(double rho, short w, const CostConsts &k)
 {
     double b = 1.0 - rho;
@@ -125,8 +187,7 @@ __device__ __forceinline__ int trunc_sigsq(double rho, short w, const CostConsts
         float lo = floorf(v - m);
         if (lo == floorf(v + m) && lo >= 0.0f && v + m < 1.0e7f) return (int)lo;
     }
-    double sigsqrho = __dmul_rn(__fma_rn(k.sigsqrhoconst, pow(b, k.rhopow), k.sigsqcorr), k.nsc2);
-    return (int)(sigsqrho / (k.costscale * (double)w));
+    return trunc_sigsq_exact(b, w, k);
 }
 
 __device__ __forceinline__ int sigsq_of(double ca, double cb, short w, const CostConsts &k)
@@ -308,6 +369,355 @@ __global__ void __launch_bounds__(256) k_costs(const float *__restrict__ ph,
     }
 }
 
+/* ── fused cost kernel, default 7 x 7 window ───────────────────────────────
+ * k_costs computes the same costs for any window; this kernel is the
+ * kperp/2 == kpar/2 == 3 case laid out for the instruction budget:
+ *  - one family per instantiation, 64 x 64 arcs per block;
+ *  - columns j and j+32 of the phase window, the differences and the row
+ *    sums are stored as float2 pairs, so every stencil step -- difference,
+ *    division by 2 pi, re-wrap, 7-term sums, division by 7 -- runs as paired
+ *    FP32 instructions (__fadd2_rn, __ffma2_rn, __fmul2_rn: IEEE
+ *    round-to-nearest per lane, the reference's per-element arithmetic);
+ *  - the per-arc cost is evaluated in FP32 with error margins (arc_fast);
+ *    the few arcs whose integer results a margin cannot decide are queued in
+ *    shared memory and finished by arc_cost's FP64 reference arithmetic
+ *    after the strip loop, by all threads of the block together.
+ * Summation order and rounding of the box-car follow cuphu_util.cu:104-181:
+ * s = 0, s += d[k] for k = 0..6, then s / 7. */
+constexpr int kC7B = 64;        /* arcs per block edge */
+constexpr int kC7W = kC7B + 6;  /* padded difference window edge */
+constexpr int kC7H = 32;        /* pairing distance: (column j, column j + 32) */
+constexpr int kC7PP = 40;       /* float2 pitch of the paired planes */
+constexpr int kC7Q = 256;       /* deferred arcs per block */
+constexpr int kC7Tab = 1024;    /* laycost table entries */
+
+struct C7Deferred {
+    float ca, cb, dp, av;
+    int rc, w;
+};
+struct C7Smem {
+    float2 php[(kC7W + 1) * kC7PP];   /* phase pairs, then the row sums */
+    float2 dpp[kC7W * kC7PP];         /* difference pairs */
+    C7Deferred q[kC7Q];
+    short lay[kC7Tab];
+    int qn;
+};
+
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+/* a - b per lane, one rounding */
+__device__ __forceinline__ float2 sub2(float2 a, float2 b)
+{
+    return __ffma2_rn(b, f2(-1.0f, -1.0f), a);
+}
+__device__ __forceinline__ float2 div_2pi2(float2 x)
+{
+    const float ax = fabsf(x.x), ay = fabsf(x.y);
+    if (ax >= 0x1p-104f && ax <= 6.6f && ay >= 0x1p-104f && ay <= 6.6f) {
+        const float2 z = f2(kRcpTwoPiRN, kRcpTwoPiRN);
+        const float2 q0 = __fmul2_rn(x, z);
+        const float2 r = __ffma2_rn(q0, f2(-kTwoPiF, -kTwoPiF), x);
+        return __ffma2_rn(r, z, q0);
+    }
+    return f2(div_2pi(x.x), div_2pi(x.y));
+}
+__device__ __forceinline__ float2 div_72(float2 x)
+{
+    const float2 z = f2(kRcp7RN, kRcp7RN);
+    const float2 q0 = __fmul2_rn(x, z);
+    const float2 r = __ffma2_rn(q0, f2(-7.0f, -7.0f), x);
+    return __ffma2_rn(r, z, q0);
+}
+/* wrap_cycles per lane: d - floorf(d + 0.5f) */
+__device__ __forceinline__ float2 wrap2(float2 d)
+{
+    const float2 t = __fadd2_rn(d, f2(0.5f, 0.5f));
+    return __ffma2_rn(f2(floorf(t.x), floorf(t.y)), f2(-1.0f, -1.0f), d);
+}
+/* (0 + v[o] + ... + v[o+6]) / 7 per lane */
+__device__ __forceinline__ float2 boxcar7(const float2 *v)
+{
+    float2 s = __fadd2_rn(f2(0.0f, 0.0f), v[0]);
+#pragma unroll
+    for (int t = 1; t < 7; ++t) s = __fadd2_rn(s, v[t]);
+    return div_72(s);
+}
+
+__device__ __forceinline__ float lg2_ftz(float x)
+{
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float ex2_ftz(float x)
+{
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+/* FP32 evaluation of arc_cost for weight 1 and coherences in [0, 1].  Each
+ * rounded decision is taken only when the FP32 value is farther from the
+ * decision boundary than the bound on its distance to the reference's FP64
+ * value, so the integers equal the reference's; otherwise returns false.
+ *  rho:    rho_f = RN(ca + cb)/2 is within 2^-23 relative of the reference's
+ *          (ca + cb)/2, so rho_f >= thresh (1 + 2^-20) and rho_f <=
+ *          thresh (1 - 2^-20) decide rho < thresh.
+ *  offset: X = RN(RN(dp - sel) nsc) is within nsc 2^-23 of the reference's
+ *          FP64 value; m_off = nsc 2^-22 + 2^-30 brackets half-integers
+ *          (DEFO, rint) or integers (SMOOTH, trunc).
+ *  sigsq:  b = ((1 - ca) + (1 - cb))/2 is within 2^-22 relative of the
+ *          reference's 1 - rho; for b >= 2^-8 the MUFU log2/exp2 estimate of
+ *          b^rhopow and the FMA stay within 2e-6 rhopow + 5e-7 relative, and
+ *          the screen (1e-5 (1 + rhopow) + 2e-6 relative + 1e-6) brackets the
+ *          truncation point with at least a 5x margin.
+ *  rho = 0 uses the exact host value of the reference's formula at b = 1. */
+template <bool DEFO>
+__device__ __forceinline__ bool arc_fast(float ca, float cb, float dp, float av,
+                                         const CostConsts &k, const short *lay, int ntab,
+                                         ArcCost &o)
+{
+    if (!(ca >= 0.0f && ca <= 1.0f && cb >= 0.0f && cb <= 1.0f)) return false;
+    const float rho = 0.5f * __fadd_rn(ca, cb);
+    const bool pos = rho >= k.thr_hi;
+    if (!pos && !(rho <= k.thr_lo)) return false;
+    const float sel = pos ? av : 0.5f * av;
+    const float X = __fmul_rn(__fsub_rn(dp, sel), k.nsc_f);
+    const float XM = __fadd_rn(X, 12582912.0f);
+    int off_i = __float_as_int(XM) - 0x4B400000;
+    const float f = __fsub_rn(X, __fsub_rn(XM, 12582912.0f));
+    if (DEFO) {
+        if (fabsf(f) > 0.5f - k.m_off) return false;
+    } else {
+        if (fabsf(f) < k.m_off) return false;
+        off_i += (f > 0.0f && X < 0.0f) ? 1 : 0;
+        off_i -= (f < 0.0f && X > 0.0f) ? 1 : 0;
+    }
+    int sg;
+    if (pos) {
+        const float b = 0.5f * __fadd_rn(1.0f - ca, 1.0f - cb);
+        if (!(b >= 0x1p-8f && b <= 1.0f)) return false;
+        const float pw = ex2_ftz(__fmul_rn(k.rhopow_f, lg2_ftz(b)));
+        const float v = __fmaf_rn(k.a_f, pw, k.c_f);
+        if (!(v >= 0.0f && v < 1.0e6f)) return false;
+        const float vm = __fadd_rn(__fsub_rn(v, 0.5f), 12582912.0f);
+        sg = __float_as_int(vm) - 0x4B400000;
+        const float fr = __fsub_rn(v, __fsub_rn(vm, 12582912.0f));
+        const float m = __fmaf_rn(k.screen_f, v, 1e-6f);
+        if (fr < m || fr > 1.0f - m) return false;
+    } else {
+        sg = k.s_rho0;
+    }
+    sg = max(sg, k.sigsqshortmin);
+    if (DEFO) {
+        if (sg >= ntab) return false;
+        o.dzmax = (short)k.dzmax;
+        o.laycost = lay[sg];
+    } else {
+        o.dzmax = 0;
+        o.laycost = 0;
+    }
+    off_i = min(max(off_i, (int)SHRT_MIN), (int)SHRT_MAX);
+    o.off = (short)off_i;
+    o.sigsq = (short)min(sg, (int)SHRT_MAX);
+    return true;
+}
+
+template <bool DEFO>
+__device__ __forceinline__ void store_arc(void *costs, size_t a, const ArcCost &o)
+{
+    if (DEFO)
+        reinterpret_cast<short4 *>(costs)[a] = make_short4(o.off, o.sigsq, o.dzmax, o.laycost);
+    else
+        reinterpret_cast<short2 *>(costs)[a] = make_short2(o.off, o.sigsq);
+}
+
+template <bool DEFO, int FAM>
+__global__ void __launch_bounds__(256, 3) k_costs7(const float *__restrict__ ph,
+                                                   const float *__restrict__ corr,
+                                                   const short *__restrict__ weights, int nrow,
+                                                   int ncol, const __grid_constant__ CostConsts k,
+                                                   void *__restrict__ costs_out, int nbx)
+{
+    extern __shared__ __align__(16) char c7raw[];
+    C7Smem &S = *reinterpret_cast<C7Smem *>(c7raw);
+    const int by = blockIdx.x / nbx, bx = blockIdx.x - (blockIdx.x / nbx) * nbx;
+    const int dr = FAM == 0 ? nrow - 1 : nrow;
+    const int dc = FAM == 0 ? ncol : ncol - 1;
+    const int r0 = by * kC7B, c0 = bx * kC7B;
+    const int tid = threadIdx.x;
+    if (tid == 0) S.qn = 0;
+    /* laycost of every sigsq the fast path can produce */
+    const int ntab = DEFO ? min(max(k.s_rho0, k.sigsqshortmin) + 1, kC7Tab) : 0;
+    if (DEFO)
+        for (int v = tid; v < ntab; v += blockDim.x)
+            S.lay[v] = (short)min(isqrt_floor(k.dzmax * v), (int)SHRT_MAX);
+
+    constexpr int NR = kC7W + (FAM == 0 ? 1 : 0);             /* phase rows */
+    constexpr int NP = kC7W - kC7H + (FAM == 1 ? 1 : 0);      /* phase pairs per row */
+    constexpr int ND = kC7W - kC7H;                            /* difference pairs per row */
+    const bool interior = r0 >= 3 && r0 + kC7B + 3 <= dr && c0 >= 3 && c0 + kC7B + 3 <= dc;
+    if (interior) {
+        /* all of a thread's window loads in flight before the first store */
+        const float *src = ph + (size_t)(r0 - 3) * ncol + (c0 - 3);
+        constexpr int NU = (NR * NP + 255) / 256;
+        float2 pv[NU];
+#pragma unroll
+        for (int t = 0; t < NU; ++t) {
+            const int u = tid + t * 256;
+            if (u < NR * NP) {
+                const int i = u / NP, j = u - (u / NP) * NP;
+                const float *row = src + (size_t)i * ncol;
+                pv[t] = f2(__ldg(row + j), __ldg(row + j + kC7H));
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < NU; ++t) {
+            const int u = tid + t * 256;
+            if (u < NR * NP) {
+                const int i = u / NP, j = u - (u / NP) * NP;
+                S.php[i * kC7PP + j] = pv[t];
+            }
+        }
+        __syncthreads();
+        for (int u = tid; u < kC7W * ND; u += blockDim.x) {
+            const int i = u / ND, j = u - (u / ND) * ND;
+            const float2 x = FAM == 0 ? sub2(S.php[i * kC7PP + j], S.php[(i + 1) * kC7PP + j])
+                                      : sub2(S.php[i * kC7PP + j + 1], S.php[i * kC7PP + j]);
+            S.dpp[i * kC7PP + j] = wrap2(div_2pi2(x));
+        }
+    } else {
+        /* window crosses the array edge: mirror-reflected differences */
+        for (int u = tid; u < kC7W * ND; u += blockDim.x) {
+            const int i = u / ND, j = u - (u / ND) * ND;
+            const int sr = reflect_index(r0 + i - 3, dr);
+            float v[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int sc = reflect_index(c0 + j + h * kC7H - 3, dc);
+                const float *p = ph + (size_t)sr * ncol + sc;
+                v[h] = wrap_cycles(FAM == 0 ? div_2pi(__fsub_rn(p[0], p[ncol]))
+                                            : div_2pi(__fsub_rn(p[1], p[0])));
+            }
+            S.dpp[i * kC7PP + j] = f2(v[0], v[1]);
+        }
+    }
+    __syncthreads();
+    /* row pass: row sums of the pairs, two pairs per thread; the sums
+     * overwrite the phase pairs ([kC7W][kC7H] pairs, pitch kC7H) */
+    float2 *tp = S.php;
+    for (int u = tid; u < kC7W * (kC7H / 2); u += blockDim.x) {
+        const int i = u >> 4, m = (u & 15) * 2;
+        const float4 *d4 = reinterpret_cast<const float4 *>(S.dpp + i * kC7PP + m);
+        float2 v[8];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const float4 q = d4[t];
+            v[2 * t] = f2(q.x, q.y);
+            v[2 * t + 1] = f2(q.z, q.w);
+        }
+        const float2 o0 = boxcar7(v), o1 = boxcar7(v + 1);
+        *reinterpret_cast<float4 *>(tp + i * kC7H + m) = make_float4(o0.x, o0.y, o1.x, o1.y);
+    }
+    __syncthreads();
+    /* column pass and arc costs: thread = column pair j, an 8-row strip
+     * walked in two halves of 4 rows */
+    const int j = tid & 31, rs0 = (tid >> 5) * 8;
+    const size_t nra = (size_t)(nrow - 1) * ncol;
+    const bool fast = k.fast != 0;
+#pragma unroll 1
+    for (int half = 0; half < 2; ++half) {
+    const int rs = rs0 + half * 4;
+    if (r0 + rs >= dr) break;
+    float2 w[10];
+#pragma unroll
+    for (int q = 0; q < 10; ++q) w[q] = tp[(rs + q) * kC7H + j];
+    /* the strip's coherence: rows rs..rs+4 (FAM 0) or columns ac, ac+1 of
+     * rows rs..rs+3 (FAM 1), loaded together */
+    float cv[2][5], cw[2][4];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int ac = c0 + j + h * kC7H;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) {
+            const int rr = r0 + rs + q;
+            cv[h][q] = 0.0f;
+            if (q < 4) cw[h][q] = 0.0f;
+            if (FAM == 0) {
+                if (ac < dc && rr < nrow) cv[h][q] = __ldg(corr + (size_t)rr * ncol + ac);
+            } else if (q < 4 && ac < dc && rr < nrow) {
+                cv[h][q] = __ldg(corr + (size_t)rr * ncol + ac);
+                cw[h][q] = __ldg(corr + (size_t)rr * ncol + ac + 1);
+            }
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        const int ar = r0 + rs + m;
+        if (ar >= dr) break;
+        const float2 avg = boxcar7(w + m);
+        const float2 dps = S.dpp[(rs + m + 3) * kC7PP + j + 3];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int ac = c0 + j + h * kC7H;
+            if (ac >= dc) continue;
+            const float dpv = h ? dps.y : dps.x, avv = h ? avg.y : avg.x;
+            size_t a;
+            float ca, cb;
+            if (FAM == 0) {
+                a = (size_t)ar * ncol + ac;
+                ca = sane(cv[h][m]);
+                cb = sane(cv[h][m + 1]);
+            } else {
+                a = nra + (size_t)ar * (ncol - 1) + ac;
+                ca = sane(cv[h][m]);
+                cb = sane(cw[h][m]);
+            }
+            const short wt = weights ? weights[a] : (short)1;
+            ArcCost o;
+            if (wt == 0) {
+                o.off = kLargeShort / 2; o.sigsq = kLargeShort;
+                o.dzmax = kLargeShort; o.laycost = 0;
+                store_arc<DEFO>(costs_out, a, o);
+            } else if (fast && wt == 1 && arc_fast<DEFO>(ca, cb, dpv, avv, k, S.lay, ntab, o)) {
+                store_arc<DEFO>(costs_out, a, o);
+            } else {
+                const int slot = atomicAdd(&S.qn, 1);
+                if (slot < kC7Q) {
+                    S.q[slot] = C7Deferred{ca, cb, dpv, avv, (ar - r0) * kC7B + (ac - c0), (int)wt};
+                } else {
+                    store_arc<DEFO>(costs_out, a,
+                                    arc_cost<DEFO>((double)ca, (double)cb, dpv, avv, wt, k));
+                }
+            }
+        }
+    }
+    }
+    __syncthreads();
+    /* deferred arcs: the reference's FP64 arithmetic, all lanes busy */
+    const int nq = min(S.qn, kC7Q);
+    for (int i = tid; i < nq; i += blockDim.x) {
+        const C7Deferred e = S.q[i];
+        const int ar = r0 + e.rc / kC7B, ac = c0 + e.rc % kC7B;
+        const size_t a = FAM == 0 ? (size_t)ar * ncol + ac : nra + (size_t)ar * (ncol - 1) + ac;
+        store_arc<DEFO>(costs_out, a,
+                        arc_cost<DEFO>((double)e.ca, (double)e.cb, e.dp, e.av, (short)e.w, k));
+    }
+}
+
+template <bool DEFO, int FAM>
+static int launch_costs7_t(const float *ph, const float *corr, const short *weights, int nrow,
+                           int ncol, const CostConsts &k, void *costs, cudaStream_t s)
+{
+    const int dr = FAM == 0 ? nrow - 1 : nrow, dc = FAM == 0 ? ncol : ncol - 1;
+    if (dr < 1 || dc < 1) return 0;
+    const int nby = (dr + kC7B - 1) / kC7B, nbx = (dc + kC7B - 1) / kC7B;
+    const size_t shm = sizeof(C7Smem);
+    CUPHU_TRY_CUDA(cudaFuncSetAttribute(k_costs7<DEFO, FAM>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+    k_costs7<DEFO, FAM><<<nby * nbx, 256, shm, s>>>(ph, corr, weights, nrow, ncol, k, costs, nbx);
+    return cuda_fail(cudaGetLastError(), "k_costs7");
+}
+
 /* ── A8 standalone ──────────────────────────────────────────────────────── */
 __global__ void __launch_bounds__(256) k_residues(const float *__restrict__ ph, int nrow,
                                                   int ncol, signed char *__restrict__ out)
@@ -450,6 +860,17 @@ int launch_costs(const float *ph, const float *corr, const short *weights, int n
     size_t pr = kCostBy + 2 * kmax, pcw = kCostBx + 2 * kmax;
     size_t shm = (pr * pcw + pr * kCostBx + (pr + 1) * (pcw + 1)) * sizeof(float);
     const bool w7 = kperp / 2 == 3 && kpar / 2 == 3;
+    if (w7) {
+        int rc = mode == CUPHU_COST_SMOOTH
+                     ? launch_costs7_t<false, 0>(ph, corr, weights, nrow, ncol, k, costs, s)
+                     : launch_costs7_t<true, 0>(ph, corr, weights, nrow, ncol, k, costs, s);
+        if (!rc)
+            rc = mode == CUPHU_COST_SMOOTH
+                     ? launch_costs7_t<false, 1>(ph, corr, weights, nrow, ncol, k, costs, s)
+                     : launch_costs7_t<true, 1>(ph, corr, weights, nrow, ncol, k, costs, s);
+        if (!rc && res) rc = launch_residues(ph, nrow, ncol, res, s);
+        return rc;
+    }
     if (mode == CUPHU_COST_SMOOTH) {
         if (w7) launch_costs_t<false, 3, 3>(nblocks, shm, s, ph, corr, weights, nrow, ncol, kperp, kpar, k, costs, res, nbx0, nby0, nbx1);
         else launch_costs_t<false, 0, 0>(nblocks, shm, s, ph, corr, weights, nrow, ncol, kperp, kpar, k, costs, res, nbx0, nby0, nbx1);

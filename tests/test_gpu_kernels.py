@@ -40,7 +40,8 @@ def gpu_costs(torch, ph, g, nlooks, mode, weights=None, kperp=7, kpar=7, residue
     return (c, to_host(dr)[: nr - 1, : nc - 1]) if residues else c
 
 
-SHAPES = [(48, 64), (33, 70), (17, 33), (5, 9), (2, 2), (1, 12), (12, 1), (130, 257)]
+SHAPES = [(48, 64), (33, 70), (17, 33), (5, 9), (2, 2), (1, 12), (12, 1), (130, 257),
+          (300, 333)]
 
 
 @pytest.mark.parametrize("shape", SHAPES)
@@ -65,7 +66,7 @@ def test_costs_windows_and_weights(torch_cuda, window):
         assert np.array_equal(got, want)
 
 
-@pytest.mark.parametrize("shape", [(48, 64), (33, 70), (130, 257)])
+@pytest.mark.parametrize("shape", [(48, 64), (33, 70), (130, 257), (300, 333)])
 @pytest.mark.parametrize("mode", [0, 1])
 def test_costs_match_reference_kernels(torch_cuda, shape, mode):
     if O.ref_lib() is None:
@@ -75,6 +76,57 @@ def test_costs_match_reference_kernels(torch_cuda, shape, mode):
     got = gpu_costs(torch_cuda, ph, g, 5.0, mode)
     ref, _ = O.ref_build_costs(ph, g, 5.0, mode=mode)
     assert np.array_equal(got, ref), f"{np.sum(np.any(got != ref, axis=1))} arcs differ"
+
+
+def test_costs_tiny_and_equal_phase_differences(torch_cuda):
+    """Phase differences that are zero, tiny or denormal take the IEEE
+    division inside the kernel; equal neighbours give exact zeros.  Costs and
+    residues must still match the oracle bit for bit, interior blocks
+    included."""
+    _, ph, g = _scene(200, 260, seed=77, nlooks=9.0)
+    ph = ph.copy()
+    ph[10:150:2, 20:200] = 0.0
+    ph[11:150:2, 20:200:3] = np.float32(1e-35)
+    ph[11:150:2, 21:200:3] = np.float32(2e-39)
+    ph[90:120, 100:180] = ph[90, 100]
+    ph[160:190, :] = np.float32(2 * np.pi) - np.float32(1e-6)
+    for mode in (0, 1):
+        got, res = gpu_costs(torch_cuda, ph, g, 9.0, mode, residues=True)
+        assert np.array_equal(got, O.build_costs(ph, g, 9.0, mode=mode))
+        assert np.array_equal(res, O.residues(ph))
+
+
+@pytest.mark.parametrize("nlooks", [1.0, 5.0, 20.0])
+def test_costs_at_decision_boundaries(torch_cuda, nlooks):
+    """Coherence at the zero-coherence threshold (to a few ulps), near 1,
+    outside [0, 1], non-finite, and weights 0/1/2: the kernels' FP32 fast
+    path must hand every arc it cannot decide to the exact arithmetic, so
+    the costs equal the oracle's bit for bit."""
+    rng = np.random.default_rng(int(nlooks))
+    nr, nc = 260, 300
+    _, ph, g = _scene(nr, nc, seed=int(nlooks) + 3, nlooks=nlooks)
+    g = g.copy()
+    thresh = 1.2 * (1.3 / nlooks + 0.14)
+    t32 = np.float32(thresh)
+    near = np.array([np.nextafter(t32, np.float32(s * 10), dtype=np.float32) if s else t32
+                     for s in (-1, 0, 1)], np.float32)
+    near = np.concatenate([near, [np.float32(thresh * (1 + 2.0 ** -21)),
+                                  np.float32(thresh * (1 - 2.0 ** -21))]]).astype(np.float32)
+    g[20:80, 10:200] = rng.choice(near, size=(60, 190))
+    g[90:110, :] = np.float32(1.0) - rng.integers(0, 400, size=(20, nc)).astype(np.float32) * 2.0 ** -24
+    g[120:125, 30:90] = np.float32(1.25)
+    g[126:128, 30:90] = np.float32(-0.5)
+    g[130, 40:60] = np.nan
+    g[131, 40:60] = np.inf
+    narcs = (nr - 1) * nc + nr * (nc - 1)
+    w = rng.choice(np.array([0, 1, 1, 1, 1, 2], np.int16), size=narcs)
+    for mode in (0, 1):
+        for weights in (None, w):
+            got = gpu_costs(torch_cuda, ph, g, nlooks, mode, weights=weights)
+            # the device reads non-finite coherence as 0, as cuphu.unwrap cleans it
+            want = O.build_costs(ph, np.where(np.isfinite(g), g, 0).astype(np.float32), nlooks,
+                                 mode=mode, weights=weights)
+            assert np.array_equal(got, want), f"{np.sum(np.any(got != want, axis=1))} arcs differ"
 
 
 def test_residues_match_oracle_and_conserve(torch_cuda):
