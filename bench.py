@@ -136,6 +136,107 @@ def cpu_baseline(ig, g, nlooks, mode, n_irls):
     return n * n / dt / 1e6, dt, int(it.sum()), n
 
 
+def adjoint_c4(seed=0, fd_arcs=0, fd_crop=256):
+    """The differentiable WLS/IRLS solve on the 2048^2 DEFO configuration
+    (5 IRLS passes): forward and backward device time of the mixed solver,
+    and the mixed gradient against the FP64 adjoint's.  Optionally central
+    finite differences (step 1e-3) on seeded random arcs, on a fd_crop^2
+    crop of the same scene solved to tol 1e-10 (Jacobi-PCG cannot reach
+    that tolerance at 2048^2 within the iteration cap, and finite
+    differences of unconverged solves measure the solver, not the
+    gradient)."""
+    import torch
+    from cuphu_b200 import synthetic as S
+    from cuphu_b200._lib import check, default_params, lib
+    from cuphu_b200.autograd import irls_solve
+    L = lib()
+    ig, g, _, ex = S.config_scene("c4_2048_defo", seed=seed)
+    nrow, ncol = g.shape
+    sptr = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    d_ig = torch.from_numpy(ig.view(np.float32)).cuda()
+    d_g = torch.from_numpy(g).cuda()
+    ph = torch.empty((nrow, ncol), dtype=torch.float32, device="cuda")
+    check(L.cuphu_phase_gpu(C.c_void_p(d_ig.data_ptr()), C.c_longlong(nrow * ncol),
+                            C.c_void_p(ph.data_ptr()), sptr))
+    narcs = (nrow - 1) * ncol + nrow * (ncol - 1)
+    cost = torch.empty((narcs, 4), dtype=torch.int16, device="cuda")
+    pc = default_params(nlooks=float(ex["nlooks"]), ncorrlooks=float(ex["nlooks"]))
+    check(L.cuphu_build_costs_device(C.c_void_p(ph.data_ptr()), C.c_void_p(d_g.data_ptr()), None,
+                                     nrow, ncol, 1, C.byref(pc), C.c_void_p(cost.data_ptr()),
+                                     None, sptr))
+    sig = cost[:, 1].to(torch.float32)
+    w = torch.where((sig > 0) & (sig < 32000), 1.0 / sig, torch.zeros_like(sig))
+    nd = (nrow - 1) * ncol
+    w0d = torch.zeros((nrow, ncol), device="cuda")
+    w0r = torch.zeros((nrow, ncol), device="cuda")
+    w0d[:-1, :] = w[:nd].view(nrow - 1, ncol)
+    w0r[:, :-1] = w[nd:].view(nrow, ncol - 1)
+    two_pi = 2 * np.pi
+    gd = torch.zeros_like(w0d)
+    gr = torch.zeros_like(w0r)
+    dd = ph[1:, :] - ph[:-1, :]
+    dr = ph[:, 1:] - ph[:, :-1]
+    gd[:-1, :] = dd - two_pi * torch.round(dd / two_pi)
+    gr[:, :-1] = dr - two_pi * torch.round(dr / two_pi)
+    c = torch.from_numpy(np.random.default_rng(seed + 1).normal(size=(nrow, ncol))).cuda()
+    n_irls = int(ex["n_irls"])
+
+    def run(prec, timing):
+        leaves = [t.clone().requires_grad_() for t in (gd, gr, w0d, w0r)]
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        torch.cuda.synchronize()
+        e[0].record()
+        u = irls_solve(*leaves, n_irls=n_irls, precision=prec)
+        loss = (c * (u - u.mean())).sum()
+        e[1].record()
+        loss.backward()
+        e[2].record()
+        torch.cuda.synchronize()
+        return ([t.grad.double() for t in leaves], e[0].elapsed_time(e[1]),
+                e[1].elapsed_time(e[2]))
+
+    run("mixed", False)                      # warm-up
+    gm, fwd_ms, bwd_ms = run("mixed", True)
+    g64, fwd64_ms, bwd64_ms = run("fp64", True)
+    rel = max(float((a - b).abs().max() / b.abs().max()) for a, b in zip(gm, g64))
+    out = {"config": "c4_2048_defo", "shape": [nrow, ncol], "n_irls": n_irls,
+           "forward_ms": fwd_ms, "backward_ms": bwd_ms, "fp64_forward_ms": fwd64_ms,
+           "fp64_backward_ms": bwd64_ms, "grad_rel_diff_mixed_vs_fp64": rel}
+    if fd_arcs:
+        rng = np.random.default_rng(seed + 2)
+        tight = dict(n_irls=n_irls, precision="fp64", max_iter=20000, tol=1e-10)
+        n = min(fd_crop, nrow, ncol)
+        gd, gr, w0d, w0r = (t[:n, :n].contiguous() for t in (gd, gr, w0d, w0r))
+        w0d[-1, :] = 0.0
+        w0r[:, -1] = 0.0
+        c = c[:n, :n].contiguous()
+        nrow = ncol = n
+        leaves = [t.clone().requires_grad_() for t in (gd, gr, w0d, w0r)]
+        u = irls_solve(*leaves, **tight)
+        (c * (u - u.mean())).sum().backward()
+        errs = []
+        for _ in range(fd_arcs):
+            k = int(rng.integers(0, 4))
+            r = int(rng.integers(0, nrow - 1 if k in (0, 2) else nrow))
+            q = int(rng.integers(0, ncol if k in (0, 2) else ncol - 1))
+            base = [t.detach() for t in (gd, gr, w0d, w0r)]
+            vals = []
+            for sgn in (1.0, -1.0):
+                pert = [t.clone() for t in base]
+                pert[k][r, q] += sgn * 1e-3
+                up = irls_solve(*pert, **tight)
+                vals.append(float((c * (up - up.mean())).sum()))
+            hp = float(np.float32(float(base[k][r, q]) + 1e-3) - np.float32(float(base[k][r, q]) - 1e-3))
+            fd = (vals[0] - vals[1]) / hp
+            gval = float(leaves[k].grad[r, q])
+            errs.append(abs(fd - gval) / max(1e-6, abs(gval), abs(fd)))
+        out["fd_arcs"] = fd_arcs
+        out["fd_crop"] = [n, n]
+        out["fd_max_rel_err"] = float(max(errs))
+        out["fd_median_rel_err"] = float(np.median(errs))
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -331,6 +432,9 @@ def run_ours(args, rank, world, local_rank):
                                 "bytes_per_px": cbytes / npix}
         del d_cost, d_ph
 
+    if rank == 0 and not args.skip_adjoint:
+        result["adjoint"] = adjoint_c4(args.seed, args.adjoint_fd)
+
     # end to end through the C ABI with pinned host buffers
     h_ig = torch.from_numpy(ig.view(np.float32)).pin_memory()
     h_g = torch.from_numpy(g).pin_memory()
@@ -392,6 +496,9 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-adjoint", action="store_true")
+    ap.add_argument("--adjoint-fd", type=int, default=0,
+                    help="finite-difference check of the adjoint on this many random arcs")
     ap.add_argument("--scale", type=int, default=None,
                     help="edge length override of the workload (small profiling cases)")
     ap.add_argument("--cost-only", action="store_true",

@@ -123,9 +123,9 @@ SIGNATURES = {
     "cuphu_conncomp_gpu": (_I, [VP, VP, VP, _I, _I, VP, VP, P(CuPhuParams), _I, VP]),
     "cuphu_conncomp_ex": (_I, [VP, VP, VP, _I, _I, C.c_float, _D, _L, _I, VP]),
     "cuphu_incrcost_early_exit": (_I, [VP, VP, _I, _L, _I, VP, VP, VP]),
-    "cuphu_wls_solve_device": (_I, [VP, VP, VP, VP, _I, _I, _I, _D, VP, VP, VP]),
-    "cuphu_wls_adjoint_device": (_I, [VP, VP, VP, VP, VP, VP, _I, _I, _I, _D, VP, VP, VP,
-                                      VP, VP, VP]),
+    "cuphu_wls_solve_device": (_I, [VP, VP, VP, VP, VP, VP, _I, _I, P(CuPhuSolveOptions), VP,
+                                    P(CuPhuSolveStats), VP]),
+    "cuphu_wls_grad_device": (_I, [VP, VP, VP, VP, VP, VP, _I, _I, VP, VP, VP, VP, VP]),
     "cuphu_gpu_count": (_I, []),
     "cuphu_gpu_name": (_I, [_I, C.c_char_p, _I]),
     "cuphu_gpu_info": (_I, [_I, P(C.c_longlong), P(_I), P(_I), P(_I)]),

@@ -258,7 +258,84 @@ struct JobOpts {
     int cost_stride = 2;
     int32_t *cycles_out = nullptr;
     float *cont_out = nullptr;      /* anchored continuous solution (single tile) */
+    /* WLS mode (single tile): caller's per-arc weights and targets or
+     * right-hand side, optional FP64 warm start, raw FP64 solution out */
+    bool wls = false;
+    const float *wls_gd = nullptr, *wls_gr = nullptr, *wls_rhs = nullptr;
+    const float *wls_wd = nullptr, *wls_wr = nullptr;
+    const double *wls_u0 = nullptr;
+    double *wls_u = nullptr;
 };
+
+/* WLS mode of run_job: copy the caller's planes into the tile layout, one
+ * solve without reweighting, raw FP64 solution out. */
+static int wls_job(const Plan &pl, SolverPlanes &P, const JobOpts &jo, cudaStream_t s,
+                   TileDesc *d_tiles, int *d_item, int ntiles, TileState *d_st, double *d_part,
+                   SolverCtl *d_ctl, float *d_deltas, int *d_pass, int dev, Workspace *W,
+                   CuPhuSolveStats *stats)
+{
+    const TileDesc &T = pl.tiles[0];
+    const size_t sp_b = (size_t)T.pitch * 4, sc_b = (size_t)T.nc * 4;
+    auto put = [&](float *dst, const float *src) -> cudaError_t {
+        return cudaMemcpy2DAsync(dst, sp_b, src, sc_b, sc_b, T.nr, cudaMemcpyDeviceToDevice, s);
+    };
+    const size_t np = (size_t)pl.nplane;
+    /* weights: zero the padding, then the caller's planes (also as w0) */
+    CUPHU_TRY_CUDA(cudaMemsetAsync(P.wd, 0, np * 4, s));
+    CUPHU_TRY_CUDA(cudaMemsetAsync(P.wr, 0, np * 4, s));
+    CUPHU_TRY_CUDA(put(P.wd, jo.wls_wd));
+    CUPHU_TRY_CUDA(put(P.wr, jo.wls_wr));
+    CUPHU_TRY_CUDA(put(P.w0d, jo.wls_wd));
+    CUPHU_TRY_CUDA(put(P.w0r, jo.wls_wr));
+    if (P.gd) CUPHU_TRY_CUDA(put((float *)P.gd, jo.wls_gd));
+    if (P.gr) CUPHU_TRY_CUDA(put((float *)P.gr, jo.wls_gr));
+    if (P.rhs) CUPHU_TRY_CUDA(put((float *)P.rhs, jo.wls_rhs));
+    if (jo.wls_u0) {
+        CUPHU_TRY_CUDA(cudaMemcpy2DAsync(P.x, (size_t)T.pitch * 8, jo.wls_u0, (size_t)T.nc * 8,
+                                         (size_t)T.nc * 8, T.nr, cudaMemcpyDeviceToDevice, s));
+        if (P.dx) CUPHU_TRY_CUDA(cudaMemsetAsync(P.dx, 0, np * 4, s));
+    }
+    const CuPhuSolveOptions &o = jo.so;
+    SolveParams sp;
+    sp.n_irls = 0;
+    sp.max_iter = o.max_iter;
+    sp.replace_every = jo.fp64 ? 0 : o.replace_every;
+    sp.tol = o.tol;
+    sp.deltas = d_deltas;
+    sp.pass_iters = d_pass;
+    sp.timeout_ns = (long long)std::max(1, o.timeout_ms) * 1000000LL;
+    sp.wls = 1;
+    sp.warm = jo.wls_u0 ? 1 : 0;
+    cudaEvent_t e1 = nullptr, e2 = nullptr;
+    if (stats) {
+        cudaEventCreate(&e1); cudaEventCreate(&e2);
+        cudaEventRecord(e1, s);
+    }
+    int rc = launch_solve(jo.fp64, d_tiles, d_item, pl.nitems, ntiles, P, pl.pitch, pl.total_rows,
+                          d_st, d_part, d_ctl, sp, dev, s);
+    if (rc) return rc;
+    CUPHU_TRY_CUDA(cudaMemcpy2DAsync(jo.wls_u, (size_t)T.nc * 8, P.x, (size_t)T.pitch * 8,
+                                     (size_t)T.nc * 8, T.nr, cudaMemcpyDeviceToDevice, s));
+    CUPHU_TRY_CUDA(cudaMemcpyAsync(W->status, &d_ctl->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CUPHU_TRY_CUDA(cudaEventRecord(W->done, s));
+    if (stats) {
+        cudaEventRecord(e2, s);
+        CUPHU_TRY_CUDA(cudaEventSynchronize(e2));
+        SolverCtl ctl;
+        CUPHU_TRY_CUDA(cudaMemcpy(&ctl, d_ctl, sizeof(ctl), cudaMemcpyDeviceToHost));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e1, e2);
+        stats->ntiles = ntiles;
+        stats->total_iters = ctl.total_iters;
+        stats->max_iters_pass = ctl.max_pass_iters;
+        stats->solve_ms = ms;
+        stats->total_ms = ms;
+        stats->px_iters = (double)ctl.px_iters;
+        cudaEventDestroy(e1); cudaEventDestroy(e2);
+        if (ctl.err) return fail(CUPHU_ERR_TIMEOUT, "solver grid barrier timed out");
+    }
+    return 0;
+}
 
 /* Enqueue the whole unwrapping pipeline for a list of scenes on stream s. */
 static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpts &jo,
@@ -303,6 +380,11 @@ static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpt
         P.cont = jo.cont_out ? b.take<float>(np) : nullptr;
         P.cc = b.take<uint32_t>(np);
         P.aux = b.take<uint32_t>(np);
+        if (jo.wls) {
+            P.gd = jo.wls_gd ? b.take<float>(np) : nullptr;
+            P.gr = jo.wls_gr ? b.take<float>(np) : nullptr;
+            P.rhs = jo.wls_rhs ? b.take<float>(np) : nullptr;
+        }
         d_tiles = b.take<TileDesc>(ntiles);
         d_item = b.take<int>(pl.nitems);
         d_sc = b.take<ScenePlan>(nsc);
@@ -403,6 +485,8 @@ static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpt
     CUPHU_TRY_CUDA(cudaMemsetAsync(d_part + 2 * (size_t)pl.nitems + 2 * (size_t)ntiles, 0,
                                    (size_t)ntiles * sizeof(double), s));
 
+    if (jo.wls) return wls_job(pl, P, jo, s, d_tiles, d_item, ntiles, d_st, d_part, d_ctl,
+                               d_deltas, d_pass, dev, W, stats);
     for (int i = 0; i < nsc; ++i) {
         if (S[i].ph_in) continue;
         long long n = (long long)S[i].nrow * S[i].ncol;
@@ -965,6 +1049,57 @@ int cuphu_laplace_solve_device(const void *d_costs, int cost_stride_shorts, cons
     jo.cost_stride = cost_stride_shorts;
     jo.cont_out = d_cont;
     return run_job(S, p, jo, (cudaStream_t)stream, stats);
+}
+
+int cuphu_wls_solve_device(const float *d_gd, const float *d_gr, const float *d_rhs,
+                           const float *d_wd, const float *d_wr, const double *d_u0, int nrow,
+                           int ncol, const CuPhuSolveOptions *opts, double *d_u,
+                           CuPhuSolveStats *stats, void *stream)
+{
+    if (!d_wd || !d_wr || !d_u || nrow < 1 || ncol < 1)
+        return fail(CUPHU_ERR_INVALID, "bad arguments");
+    const bool have_g = d_gd != nullptr || d_gr != nullptr;
+    if (have_g == (d_rhs != nullptr))
+        return fail(CUPHU_ERR_INVALID, "give either the arc targets (gd, gr) or a right-hand side");
+    if (have_g && (!d_gd || !d_gr))
+        return fail(CUPHU_ERR_INVALID, "gd and gr are both required");
+    CuPhuParams p;
+    cuphu_default_params(&p);
+    CuPhuSolveOptions so;
+    if (opts) so = *opts; else default_solve_options(&so);
+    SceneIn in;
+    in.ph_in = have_g ? d_gd : d_rhs;   /* any nrow x ncol plane: the phase is not read */
+    in.corr = d_wd;
+    in.nrow = nrow;
+    in.ncol = ncol;
+    in.nlooks = p.ncorrlooks;
+    std::vector<SceneIn> S(1, in);
+    JobOpts jo;
+    jo.fp64 = so.precision == CUPHU_PREC_FP64;
+    jo.so = so;
+    jo.so.n_irls = 0;
+    jo.want_cc = false;
+    jo.wls = true;
+    jo.wls_gd = d_gd;
+    jo.wls_gr = d_gr;
+    jo.wls_rhs = d_rhs;
+    jo.wls_wd = d_wd;
+    jo.wls_wr = d_wr;
+    jo.wls_u0 = d_u0;
+    jo.wls_u = d_u;
+    return run_job(S, p, jo, (cudaStream_t)stream, stats);
+}
+
+int cuphu_wls_grad_device(const double *d_lambda, const double *d_u, const float *d_gd,
+                          const float *d_gr, const float *d_wd, const float *d_wr, int nrow,
+                          int ncol, double *d_ggd, double *d_ggr, double *d_gwd, double *d_gwr,
+                          void *stream)
+{
+    if (!d_lambda || !d_u || !d_gd || !d_gr || !d_wd || !d_wr || !d_ggd || !d_ggr || !d_gwd ||
+        !d_gwr || nrow < 1 || ncol < 1)
+        return fail(CUPHU_ERR_INVALID, "bad arguments");
+    return launch_wls_grad(d_lambda, d_u, d_gd, d_gr, d_wd, d_wr, nrow, ncol, d_ggd, d_ggr, d_gwd,
+                           d_gwr, (cudaStream_t)stream);
 }
 
 int cuphu_laplace_unwrap_gpu(const void *d_smooth_costs, const float *d_phase, int nrow, int ncol,

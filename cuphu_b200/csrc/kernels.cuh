@@ -46,6 +46,9 @@ struct SolverPlanes {
     float *cont;                /* optional anchored continuous solution */
     uint32_t *cc;               /* union-find parents, then labels       */
     uint32_t *aux;              /* component sizes, then root labels     */
+    const float *gd, *gr;       /* WLS mode: per-arc targets in place of the
+                                   wrapped phase differences (optional) */
+    const float *rhs;           /* WLS mode: explicit right-hand side (optional) */
 };
 
 /* per-tile PCG scalars, double-buffered by iteration parity: every block
@@ -68,6 +71,8 @@ struct SolveParams {
     const float *deltas;        /* per-pass IRLS delta (host powf schedule) */
     int *pass_iters;            /* [n_irls+1] iterations per pass (out)     */
     long long timeout_ns;       /* grid-barrier wait limit                   */
+    int wls = 0;                /* raw solve: no anchor / congruence phase   */
+    int warm = 0;               /* keep the caller's initial x on pass 0     */
 };
 
 struct ScenePlan {
@@ -132,6 +137,11 @@ int launch_stitch(const ScenePlan *scenes, int nscenes, const TileDesc *tiles,
 int launch_merge(const ScenePlan *scenes, const ScenePlan *h_scenes, int nscenes,
                  const TileDesc *tiles, const SolverPlanes &P, const double *tile_k,
                  const unsigned *comp_off, const SceneOut *sout, cudaStream_t s);
+
+/* adjoint.cu */
+int launch_wls_grad(const double *lam, const double *u, const float *gd, const float *gr,
+                    const float *wd, const float *wr, int nrow, int ncol, double *ggd, double *ggr,
+                    double *gwd, double *gwr, cudaStream_t s);
 
 /* integrate.cu */
 int launch_integrate(const float *ph, const short *hflows, const short *vflows, int nrow,

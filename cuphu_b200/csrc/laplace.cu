@@ -214,6 +214,9 @@ __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, b
     V *dg = (V *)P.diag + T.pix;
     const float *wd = P.wd + T.pix, *wr = P.wr + T.pix;
     const float *ph = T.ph;
+    /* WLS mode: per-arc targets or an explicit right-hand side */
+    const float *gdp = P.gd ? P.gd + T.pix : nullptr, *grp = P.gr ? P.gr + T.pix : nullptr;
+    const float *rhsp = P.rhs ? P.rhs + T.pix : nullptr;
     const double eps = (double)kLapEpsF;
     const int r = q.r, nr = T.nr, nc = T.nc, pitch = T.pitch, pp = T.ph_pitch;
     size_t prow = (size_t)r * pitch;
@@ -233,12 +236,12 @@ __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, b
             continue;
         }
         size_t gi = (size_t)r * pp + c, pi = prow + c;
-        float pa = __ldg(ph + gi);
+        float pa = gdp ? 0.0f : __ldg(ph + gi);
         double bv = 0.0, ws = 0.0;
         if (r < nr - 1) {
             float w = ldc(wd + pi);
             if (w > 0.0f) {
-                float g = lap_wrap_pi(__ldg(ph + gi + pp) - pa);
+                float g = gdp ? ldc(gdp + pi) : lap_wrap_pi(__ldg(ph + gi + pp) - pa);
                 bv = __fma_rn(-(double)w, (double)g, bv);
                 ws += w;
             }
@@ -246,7 +249,7 @@ __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, b
         if (r > 0) {
             float w = ldc(wd + pi - pitch);
             if (w > 0.0f) {
-                float g = lap_wrap_pi(pa - __ldg(ph + gi - pp));
+                float g = gdp ? ldc(gdp + pi - pitch) : lap_wrap_pi(pa - __ldg(ph + gi - pp));
                 bv = __fma_rn((double)w, (double)g, bv);
                 ws += w;
             }
@@ -254,7 +257,7 @@ __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, b
         if (c < nc - 1) {
             float w = ldc(wr + pi);
             if (w > 0.0f) {
-                float g = lap_wrap_pi(__ldg(ph + gi + 1) - pa);
+                float g = grp ? ldc(grp + pi) : lap_wrap_pi(__ldg(ph + gi + 1) - pa);
                 bv = __fma_rn(-(double)w, (double)g, bv);
                 ws += w;
             }
@@ -262,11 +265,12 @@ __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, b
         if (c > 0) {
             float w = ldc(wr + pi - 1);
             if (w > 0.0f) {
-                float g = lap_wrap_pi(pa - __ldg(ph + gi - 1));
+                float g = grp ? ldc(grp + pi - 1) : lap_wrap_pi(pa - __ldg(ph + gi - 1));
                 bv = __fma_rn((double)w, (double)g, bv);
                 ws += w;
             }
         }
+        if (rhsp) bv = (double)ldc(rhsp + pi);
         double d = write_diag ? ws + eps : (double)dv[j];
         double y;
         if (zero_x) {
@@ -1144,7 +1148,7 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
             int a, b;
             slice_items(sc, T, t, a, b);
             for (int li = a; li < b; ++li)
-                store_partial(phase_init<V>(T, li, P, outer == 0, true), pbuf[pc & 1],
+                store_partial(phase_init<V>(T, li, P, outer == 0 && !sp.warm, true), pbuf[pc & 1],
                               T.item0 + li, sw);
             if (b > a) seg_done(T, t, b - a, pbuf[pc & 1], tbuf[pc & 1], tick, sw, &s_bcast, &s_flag);
         }
@@ -1319,6 +1323,7 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
             if (!grid_sync(ctl, timeout_ns)) return;
         }
     }
+    if (sp.wls) return;   /* WLS mode: the caller reads the raw solution x */
     setup_slice(sc, tiles, nullptr, ntiles, sw);
     for (int t = sc.t0; t <= sc.t1; ++t) {
         const TileDesc &T = stile(sc, tiles, t);

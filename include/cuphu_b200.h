@@ -257,6 +257,31 @@ int cuphu_laplace_solve_device(const void *d_costs, int cost_stride_shorts,
                                int32_t *d_cycles, float *d_cont, CuPhuSolveStats *stats,
                                void *stream);
 
+/* ── weighted least-squares solve and its adjoint (new; the differentiable
+ *    core of the Laplace path, cuphu_laplace.cu:88-190 with explicit inputs)
+ * u = argmin_u sum_a w_a ((D u)_a - g_a)^2 + eps |u|^2 on one nrow x ncol
+ * grid, i.e. (D^T W D + eps I) u = D^T W g with eps = 1e-12 (the Laplace
+ * solver's operator).  Planes are nrow x ncol, row-major, device memory:
+ * d_gd/d_wd hold arc (r,c)->(r+1,c) (last row ignored), d_gr/d_wr arc
+ * (r,c)->(r,c+1) (last column ignored); (D u)_a = u(head) - u(tail).
+ * Give either d_gd and d_gr, or d_rhs (nrow x ncol) to solve
+ * (D^T W D + eps I) u = rhs -- the adjoint solve.  d_u0: optional FP64
+ * warm start.  d_u: FP64 solution (no anchoring).  opts: precision,
+ * max_iter, tol, replace_every, timeout_ms (n_irls is ignored). */
+int cuphu_wls_solve_device(const float *d_gd, const float *d_gr, const float *d_rhs,
+                           const float *d_wd, const float *d_wr, const double *d_u0, int nrow,
+                           int ncol, const CuPhuSolveOptions *opts, double *d_u,
+                           CuPhuSolveStats *stats, void *stream);
+
+/* gradients of the WLS solve from the adjoint state lambda = (D^T W D +
+ * eps I)^-1 ubar and the forward solution u: d_ggd/d_ggr = w (D lambda),
+ * d_gwd/d_gwr = (D lambda)(g - D u); nrow x ncol FP64 planes laid out like
+ * the inputs (unused last row / column written 0) */
+int cuphu_wls_grad_device(const double *d_lambda, const double *d_u, const float *d_gd,
+                          const float *d_gr, const float *d_wd, const float *d_wr, int nrow,
+                          int ncol, double *d_ggd, double *d_ggr, double *d_gwd, double *d_gwr,
+                          void *stream);
+
 /* ── integration of MCF flows (ref cuphu.h:261-270, cuphu_phase.cu:110-144) */
 int cuphu_integrate_phase_gpu(const float *wrapped_phase, const short *hflows,
                               const short *vflows, int nrow, int ncol, int gpu_id,
