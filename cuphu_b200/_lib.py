@@ -125,6 +125,10 @@ SIGNATURES = {
     "cuphu_incrcost_early_exit": (_I, [VP, VP, _I, _L, _I, VP, VP, VP]),
     "cuphu_wls_solve_device": (_I, [VP, VP, VP, VP, VP, VP, _I, _I, P(CuPhuSolveOptions), VP,
                                     P(CuPhuSolveStats), VP]),
+    "cuphu_batch_graph_create": (_I, [P(CuPhuScene), _I, _I, P(CuPhuParams), P(CuPhuSolveOptions),
+                                      P(VP)]),
+    "cuphu_batch_graph_launch": (_I, [VP, VP]),
+    "cuphu_batch_graph_destroy": (_I, [VP]),
     "cuphu_wls_grad_device": (_I, [VP, VP, VP, VP, VP, VP, _I, _I, VP, VP, VP, VP, VP]),
     "cuphu_gpu_count": (_I, []),
     "cuphu_gpu_name": (_I, [_I, C.c_char_p, _I]),

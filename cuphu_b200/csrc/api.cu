@@ -58,10 +58,8 @@ struct Workspace {
 
 static Workspace g_ws[64];
 
-static int ws_acquire(int dev, size_t dbytes, size_t hbytes, cudaStream_t s, Workspace *&W)
+static int ws_prepare(Workspace *W, size_t dbytes, size_t hbytes, cudaStream_t s)
 {
-    if (dev < 0 || dev >= 64) return fail(CUPHU_ERR_INVALID, "device index out of range");
-    W = &g_ws[dev];
     if (!W->done) {
         CUPHU_TRY_CUDA(cudaEventCreateWithFlags(&W->done, cudaEventDisableTiming));
         CUPHU_TRY_CUDA(cudaEventRecord(W->done, s));
@@ -102,6 +100,31 @@ static int ws_acquire(int dev, size_t dbytes, size_t hbytes, cudaStream_t s, Wor
     CUPHU_TRY_CUDA(cudaEventSynchronize(W->done));
     return 0;
 }
+
+static int ws_acquire(int dev, size_t dbytes, size_t hbytes, cudaStream_t s, Workspace *&W)
+{
+    if (dev < 0 || dev >= 64) return fail(CUPHU_ERR_INVALID, "device index out of range");
+    W = &g_ws[dev];
+    return ws_prepare(W, dbytes, hbytes, s);
+}
+
+static void ws_free(Workspace &W)
+{
+    if (W.dev) cudaFree(W.dev);
+    if (W.host) cudaFreeHost(W.host);
+    if (W.status) cudaFreeHost(W.status);
+    if (W.done) cudaEventDestroy(W.done);
+    W.dev = nullptr; W.host = nullptr; W.status = nullptr; W.done = nullptr;
+    W.dev_size = W.host_size = 0;
+}
+
+/* a captured batch pipeline: its own workspace (the descriptors and device
+ * pointers are baked into the graph) and the instantiated graph */
+struct GraphJob {
+    Workspace ws;
+    cudaGraphExec_t exec = nullptr;
+    int dev = 0;
+};
 
 struct Bump {
     char *base;
@@ -260,6 +283,7 @@ struct JobOpts {
     float *cont_out = nullptr;      /* anchored continuous solution (single tile) */
     /* WLS mode (single tile): caller's per-arc weights and targets or
      * right-hand side, optional FP64 warm start, raw FP64 solution out */
+    GraphJob *graph = nullptr;      /* capture mode: leave the capture open on s */
     bool wls = false;
     const float *wls_gd = nullptr, *wls_gr = nullptr, *wls_rhs = nullptr;
     const float *wls_wd = nullptr, *wls_wr = nullptr;
@@ -425,9 +449,16 @@ static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpt
     size_t desc_end = (size_t)((char *)d_st - (char *)nullptr);
     size_t hbytes = desc_end - desc_begin + 256;
 
-    std::lock_guard<std::mutex> lock(g_ws[dev].mu);
+    std::unique_lock<std::mutex> lock;
     Workspace *W = nullptr;
-    rc = ws_acquire(dev, dbytes, hbytes, s, W);
+    if (jo.graph) {
+        if (stats) return fail(CUPHU_ERR_INVALID, "statistics are not available in a graph");
+        W = &jo.graph->ws;
+        rc = ws_prepare(W, dbytes, hbytes, s);
+    } else {
+        lock = std::unique_lock<std::mutex>(g_ws[dev].mu);
+        rc = ws_acquire(dev, dbytes, hbytes, s, W);
+    }
     if (rc) return rc;
     Bump b(W->dev);
     layout(b, P, phase, d_tiles, d_item, d_sc, d_pairs, d_maps, d_rowcnt, d_nlab, d_pairk, d_tilek,
@@ -472,14 +503,24 @@ static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpt
         cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2); cudaEventCreate(&e3);
         cudaEventRecord(e0, s);
     }
-    CUPHU_TRY_CUDA(cudaMemcpyAsync(d_tiles, h, (char *)d_st - (char *)d_tiles,
-                                   cudaMemcpyHostToDevice, s));
     /* IRLS schedule, host powf exactly as cuphu_laplace.cu:517-518 */
     std::vector<float> deltas(o.n_irls + 1, 0.0f);
     for (int k = 0; k < o.n_irls; ++k)
         deltas[k] = std::max(o.irls_delta_min, o.irls_delta_max * powf(0.5f, (float)k));
-    CUPHU_TRY_CUDA(cudaMemcpyAsync(d_deltas, deltas.data(), deltas.size() * sizeof(float),
-                                   cudaMemcpyHostToDevice, s));
+    if (jo.graph) {
+        /* the graph replays everything after the descriptors: upload them
+         * now, then capture the rest */
+        CUPHU_TRY_CUDA(cudaMemcpy(d_tiles, h, (char *)d_st - (char *)d_tiles,
+                                  cudaMemcpyHostToDevice));
+        CUPHU_TRY_CUDA(cudaMemcpy(d_deltas, deltas.data(), deltas.size() * sizeof(float),
+                                  cudaMemcpyHostToDevice));
+        CUPHU_TRY_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+    } else {
+        CUPHU_TRY_CUDA(cudaMemcpyAsync(d_tiles, h, (char *)d_st - (char *)d_tiles,
+                                       cudaMemcpyHostToDevice, s));
+        CUPHU_TRY_CUDA(cudaMemcpyAsync(d_deltas, deltas.data(), deltas.size() * sizeof(float),
+                                       cudaMemcpyHostToDevice, s));
+    }
     CUPHU_TRY_CUDA(cudaMemsetAsync(d_st, 0, 2 * ntiles * sizeof(TileState), s));
     CUPHU_TRY_CUDA(cudaMemsetAsync(d_ctl, 0, sizeof(SolverCtl), s));
     CUPHU_TRY_CUDA(cudaMemsetAsync(d_part + 2 * (size_t)pl.nitems + 2 * (size_t)ntiles, 0,
@@ -543,6 +584,7 @@ static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpt
         CUPHU_TRY_CUDA(cudaMemcpy2DAsync(jo.cont_out, (size_t)T.nc * 4, P.cont, (size_t)T.pitch * 4,
                                          (size_t)T.nc * 4, T.nr, cudaMemcpyDeviceToDevice, s));
     }
+    if (jo.graph) return 0;   /* the caller ends the capture */
     CUPHU_TRY_CUDA(cudaMemcpyAsync(W->status, &d_ctl->err, sizeof(int), cudaMemcpyDeviceToHost, s));
     CUPHU_TRY_CUDA(cudaEventRecord(W->done, s));
     if (stats) {
@@ -735,16 +777,16 @@ int cuphu_unwrap_device(const float *igram_c64, const float *phase_in, const flo
     return run_job(S, *params, jo, (cudaStream_t)stream, stats);
 }
 
-int cuphu_unwrap_batch_device(const CuPhuScene *scenes, int nscenes, CuPhuCostMode cost_mode,
-                              const CuPhuParams *params, const CuPhuSolveOptions *opts,
-                              CuPhuSolveStats *stats, void *stream)
+static int batch_scenes(const CuPhuScene *scenes, int nscenes, CuPhuCostMode cost_mode,
+                        const CuPhuParams *params, const CuPhuSolveOptions *opts,
+                        std::vector<SceneIn> &S, JobOpts &jo)
 {
     int rc = check_common(cost_mode, params);
     if (rc) return rc;
     if (!scenes || nscenes < 1) return fail(CUPHU_ERR_INVALID, "no scenes");
     CuPhuSolveOptions so;
     if (opts) so = *opts; else default_solve_options(&so);
-    std::vector<SceneIn> S(nscenes);
+    S.assign(nscenes, SceneIn());
     for (int i = 0; i < nscenes; ++i) {
         const CuPhuScene &c = scenes[i];
         if ((!c.igram_c64 && !c.phase) || !c.corr || !c.unw_out)
@@ -765,13 +807,84 @@ int cuphu_unwrap_batch_device(const CuPhuScene *scenes, int nscenes, CuPhuCostMo
         in.ref_row = so.ref_row;
         in.ref_col = so.ref_col;
     }
-    JobOpts jo;
     jo.fp64 = so.precision == CUPHU_PREC_FP64;
     jo.so = so;
     bool cc = true;
     for (auto &in : S) cc = cc && in.cc;
     jo.want_cc = cc;
+    return 0;
+}
+
+int cuphu_unwrap_batch_device(const CuPhuScene *scenes, int nscenes, CuPhuCostMode cost_mode,
+                              const CuPhuParams *params, const CuPhuSolveOptions *opts,
+                              CuPhuSolveStats *stats, void *stream)
+{
+    std::vector<SceneIn> S;
+    JobOpts jo;
+    int rc = batch_scenes(scenes, nscenes, cost_mode, params, opts, S, jo);
+    if (rc) return rc;
     return run_job(S, *params, jo, (cudaStream_t)stream, stats);
+}
+
+int cuphu_batch_graph_create(const CuPhuScene *scenes, int nscenes, CuPhuCostMode cost_mode,
+                             const CuPhuParams *params, const CuPhuSolveOptions *opts,
+                             void **graph_out)
+{
+    if (!graph_out) return fail(CUPHU_ERR_INVALID, "graph_out must not be NULL");
+    *graph_out = nullptr;
+    std::vector<SceneIn> S;
+    JobOpts jo;
+    int rc = batch_scenes(scenes, nscenes, cost_mode, params, opts, S, jo);
+    if (rc) return rc;
+    auto *G = new GraphJob();
+    CUPHU_TRY_CUDA(cudaGetDevice(&G->dev));
+    cudaStream_t s = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+        delete G;
+        return fail(CUPHU_ERR_CUDA, "stream creation failed");
+    }
+    jo.graph = G;
+    rc = run_job(S, *params, jo, s, nullptr);
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(s, &cs);
+    cudaGraph_t g = nullptr;
+    if (cs != cudaStreamCaptureStatusNone) {
+        cudaError_t e = cudaStreamEndCapture(s, &g);
+        if (!rc && e != cudaSuccess) rc = cuda_fail(e, "cudaStreamEndCapture");
+    }
+    if (!rc) {
+        cudaError_t e = cudaGraphInstantiate(&G->exec, g, 0);
+        if (e != cudaSuccess) rc = cuda_fail(e, "cudaGraphInstantiate");
+    }
+    if (g) cudaGraphDestroy(g);
+    cudaStreamDestroy(s);
+    if (rc) {
+        if (G->exec) cudaGraphExecDestroy(G->exec);
+        ws_free(G->ws);
+        delete G;
+        return rc;
+    }
+    *graph_out = G;
+    return 0;
+}
+
+int cuphu_batch_graph_launch(void *graph, void *stream)
+{
+    auto *G = static_cast<GraphJob *>(graph);
+    if (!G || !G->exec) return fail(CUPHU_ERR_INVALID, "not a graph from cuphu_batch_graph_create");
+    CUPHU_TRY_CUDA(cudaGraphLaunch(G->exec, (cudaStream_t)stream));
+    return 0;
+}
+
+int cuphu_batch_graph_destroy(void *graph)
+{
+    auto *G = static_cast<GraphJob *>(graph);
+    if (!G) return 0;
+    CUPHU_TRY_CUDA(cudaDeviceSynchronize());
+    if (G->exec) cudaGraphExecDestroy(G->exec);
+    ws_free(G->ws);
+    delete G;
+    return 0;
 }
 
 int cuphu_unwrap_ex(const float *igram_c64, const float *corr, const unsigned char *mask,

@@ -257,6 +257,20 @@ int cuphu_laplace_solve_device(const void *d_costs, int cost_stride_shorts,
                                int32_t *d_cycles, float *d_cont, CuPhuSolveStats *stats,
                                void *stream);
 
+/* ── batched pipeline as a CUDA graph (new) ─────────────────────────────────
+ * Plans the batch once into a workspace owned by the graph object, uploads
+ * its descriptors and captures the whole device pipeline (state resets,
+ * phase, weights, the persistent solve, conncomp, stitching, merge) into a
+ * CUDA graph on the current device.  Every launch re-runs that pipeline on
+ * the same device buffers named in `scenes` (refill the inputs in place
+ * between launches).  Launches of one graph must not overlap each other on
+ * the GPU.  Destroy synchronises the device and frees the workspace. */
+int cuphu_batch_graph_create(const CuPhuScene *scenes, int nscenes, CuPhuCostMode cost_mode,
+                             const CuPhuParams *params, const CuPhuSolveOptions *opts,
+                             void **graph_out);
+int cuphu_batch_graph_launch(void *graph, void *stream);
+int cuphu_batch_graph_destroy(void *graph);
+
 /* ── weighted least-squares solve and its adjoint (new; the differentiable
  *    core of the Laplace path, cuphu_laplace.cu:88-190 with explicit inputs)
  * u = argmin_u sum_a w_a ((D u)_a - g_a)^2 + eps |u|^2 on one nrow x ncol

@@ -88,6 +88,57 @@ def test_batch_matches_individual_calls(torch_cuda):
         assert np.array_equal(c, singles[i][1])
 
 
+def test_batch_graph_replays_the_batch(torch_cuda):
+    """cuphu_batch_graph_*: replaying the captured pipeline gives the batched
+    call's outputs bit for bit, twice in a row and after the inputs are
+    refilled in place."""
+    shapes = [(96, 130), (64, 64), (150, 77), (40, 200)]
+    tiles = [((2, 2), (16, 16)), ((1, 1), (0, 0)), ((2, 1), (10, 0)), ((1, 2), (0, 12))]
+    sets = []
+    for seed in (30, 40):
+        sets.append([O.phase_from_igram(S.bumps(*sh, seed=seed + i, nbumps=2, amp_range=(5, 20),
+                                                sigma_range=(8, 20))[0]) for i, sh in
+                     enumerate(shapes)])
+    gs = [S.bumps(*sh, seed=50 + i, nbumps=2)[1] for i, sh in enumerate(shapes)]
+    dph = [to_dev(a) for a in sets[0]]
+    dg = [to_dev(g) for g in gs]
+    du = [empty(sh, torch_cuda.float32) for sh in shapes]
+    dc = [empty(sh, torch_cuda.int32) for sh in shapes]
+    scenes = (CuPhuScene * len(shapes))()
+    for i, (sh, (nt, ov)) in enumerate(zip(shapes, tiles)):
+        scenes[i] = CuPhuScene(None, dph[i].data_ptr(), dg[i].data_ptr(), None, None, sh[0], sh[1],
+                               nt[0], nt[1], ov[0], ov[1], 5.0, du[i].data_ptr(), dc[i].data_ptr())
+    p = default_params()
+    o = default_solve_options(precision=0, n_irls=2)
+
+    def batch_outputs():
+        check(lib().cuphu_unwrap_batch_device(scenes, len(shapes), 0, C.byref(p), C.byref(o),
+                                              None, None))
+        return [(to_host(u).copy(), to_host(c).copy()) for u, c in zip(du, dc)]
+
+    want = [batch_outputs()]
+    for i in range(len(shapes)):
+        dph[i].copy_(to_dev(sets[1][i]))
+    want.append(batch_outputs())
+    for i in range(len(shapes)):
+        dph[i].copy_(to_dev(sets[0][i]))
+    graph = C.c_void_p()
+    check(lib().cuphu_batch_graph_create(scenes, len(shapes), 0, C.byref(p), C.byref(o),
+                                         C.byref(graph)))
+    try:
+        for k in (0, 0, 1):
+            for i in range(len(shapes)):
+                dph[i].copy_(to_dev(sets[k][i]))
+                du[i].fill_(float("nan"))
+            stream = torch_cuda.cuda.current_stream().cuda_stream
+            check(lib().cuphu_batch_graph_launch(graph, C.c_void_p(stream)))
+            for i in range(len(shapes)):
+                assert np.array_equal(to_host(du[i]).view(np.int32), want[k][i][0].view(np.int32))
+                assert np.array_equal(to_host(dc[i]), want[k][i][1])
+    finally:
+        check(lib().cuphu_batch_graph_destroy(graph))
+
+
 def test_reference_pixel_shift_and_cc_on_device(torch_cuda):
     ig, g, _, _ = S.bumps(90, 110, seed=8, nbumps=2, amp_range=(10, 30), sigma_range=(10, 30))
     ph = O.phase_from_igram(ig)
