@@ -386,6 +386,11 @@ def run_ours(args, rank, world, local_rank):
     if "n_irls" in ex:
         opts.n_irls = int(ex["n_irls"])
 
+    tuned = None
+    if not (args.profile or args.cost_only or args.no_autotune):
+        import cuphu_b200
+        tuned = cuphu_b200.autotune(ig, g, nlooks, cost=ex["cost"], ntiles=(ntr, ntc),
+                                    tile_overlap=(64, 64), gpu_id=local_rank)
     d_ig = torch.from_numpy(ig.view(np.float32)).cuda()
     d_g = torch.from_numpy(g).cuda()
     d_u = torch.empty((nrow, ncol), dtype=torch.float32, device="cuda")
@@ -578,7 +583,7 @@ def run_ours(args, rank, world, local_rank):
                            "tiles": [ntr, ntc], "overlap": 64, "n_irls": opts.n_irls,
                            "max_iter": opts.max_iter, "tol": opts.tol,
                            "precision": args.precision, "parallelism": f"replicas{world}",
-                           "l2": "inputs (805 MB) larger than L2"},
+                           "l2": "inputs (805 MB) larger than L2", "autotune": tuned},
                 "e2e": {"value": world * npix / e2e_s / 1e6, "unit": "Mpix/s",
                         "h2d_bytes_per_step": npix * 12, "d2h_bytes_per_step": npix * 8},
                 "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
@@ -599,6 +604,7 @@ def main():
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-adjoint", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--adjoint-fd", type=int, default=0,
                     help="finite-difference check of the adjoint on this many random arcs")
     ap.add_argument("--scale", type=int, default=None,

@@ -9,9 +9,10 @@ components and flow integration run as hand-written CUDA kernels in
 from cuphu_b200._conncomp import regrow_conncomp
 from cuphu_b200._gpu import gpu_count, gpu_info, gpu_name
 from cuphu_b200._looks import get_effective_looks
+from cuphu_b200._tune import autotune
 from cuphu_b200._unwrap import unwrap
 
 __version__ = "0.1.0"
 
-__all__ = ["__version__", "get_effective_looks", "gpu_count", "gpu_info", "gpu_name",
-           "regrow_conncomp", "unwrap"]
+__all__ = ["__version__", "autotune", "get_effective_looks", "gpu_count", "gpu_info",
+           "gpu_name", "regrow_conncomp", "unwrap"]

@@ -125,6 +125,7 @@ SIGNATURES = {
     "cuphu_incrcost_early_exit": (_I, [VP, VP, _I, _L, _I, VP, VP, VP]),
     "cuphu_wls_solve_device": (_I, [VP, VP, VP, VP, VP, VP, _I, _I, P(CuPhuSolveOptions), VP,
                                     P(CuPhuSolveStats), VP]),
+    "cuphu_autotune": (_I, [VP, VP, _I, _I, _I, P(CuPhuParams), P(CuPhuTileParams), _I, P(_I)]),
     "cuphu_batch_graph_create": (_I, [P(CuPhuScene), _I, _I, P(CuPhuParams), P(CuPhuSolveOptions),
                                       P(VP)]),
     "cuphu_batch_graph_launch": (_I, [VP, VP]),

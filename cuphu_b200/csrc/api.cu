@@ -887,6 +887,80 @@ int cuphu_batch_graph_destroy(void *graph)
     return 0;
 }
 
+int cuphu_autotune(const float *igram_c64, const float *corr, int nrow, int ncol,
+                   CuPhuCostMode cost_mode, const CuPhuParams *params,
+                   const CuPhuTileParams *tile, int gpu_id, int *choices)
+{
+    int rc = check_common(cost_mode, params);
+    if (rc) return rc;
+    if (!igram_c64 || !corr || nrow < 2 || ncol < 2)
+        return fail(CUPHU_ERR_INVALID, "igram and corr of at least 2x2 pixels are required");
+    CUPHU_TRY_CUDA(cudaSetDevice(gpu_id));
+    cudaStream_t s = lib_stream(gpu_id);
+    const size_t n = (size_t)nrow * ncol;
+    const size_t narcs = (size_t)(nrow - 1) * ncol + (size_t)nrow * (ncol - 1);
+    const int es = cost_mode == CUPHU_COST_SMOOTH ? 2 : 4;
+    float *d_ig = dev_alloc_async<float>(2 * n, s), *d_corr = dev_alloc_async<float>(n, s);
+    float *d_ph = dev_alloc_async<float>(n, s), *d_unw = dev_alloc_async<float>(n, s);
+    short *d_cost = dev_alloc_async<short>(narcs * es, s);
+    if (!d_ig || !d_corr || !d_ph || !d_unw || !d_cost) rc = fail(CUPHU_ERR_ALLOC, "device allocation failed");
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int best_cost = 0, best_blocks = 3;
+    if (!rc) {
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaMemcpyAsync(d_ig, igram_c64, 8 * n, cudaMemcpyHostToDevice, s);
+        cudaMemcpyAsync(d_corr, corr, 4 * n, cudaMemcpyHostToDevice, s);
+        rc = launch_phase(reinterpret_cast<const float2 *>(d_ig), d_ph, (long long)n, s);
+    }
+    /* cost kernel: 3 or 4 blocks per SM (identical results) */
+    float best_ms = 1e30f;
+    for (int v = 0; v < 2 && !rc; ++v) {
+        tune_force(0, v);
+        for (int rep = 0; rep < 2 && !rc; ++rep) {
+            cudaEventRecord(e0, s);
+            for (int k = 0; k < 3 && !rc; ++k)
+                rc = launch_costs(d_ph, d_corr, nullptr, nrow, ncol,
+                                  cost_mode == CUPHU_COST_SMOOTH ? 0 : 1, *params, d_cost,
+                                  nullptr, s);
+            cudaEventRecord(e1, s);
+            cudaEventSynchronize(e1);
+        }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) { best_ms = ms; best_cost = v; }
+    }
+    tune_force(0, -1);
+    if (!rc) tune_set(gpu_id, 0, 2LL * nrow * ncol, best_cost);
+    /* persistent solver: 2 or 3 blocks per SM, 20 PCG iterations, no IRLS */
+    best_ms = 1e30f;
+    long long items = 0;
+    for (int per_sm = 2; per_sm <= 3 && !rc; ++per_sm) {
+        tune_force(1, per_sm);
+        CuPhuSolveOptions so;
+        default_solve_options(&so);
+        so.max_iter = 20;
+        so.n_irls = 0;
+        so.ref_row = so.ref_col = -1;
+        CuPhuSolveStats st = {};
+        for (int rep = 0; rep < 2 && !rc; ++rep)
+            rc = cuphu_unwrap_device(nullptr, d_ph, d_corr, nullptr, nullptr, nrow, ncol, cost_mode,
+                                     params, tile, &so, d_unw, nullptr, nullptr, &st, s);
+        items = tune_probe_items();
+        if (!rc && st.solve_ms < best_ms) { best_ms = (float)st.solve_ms; best_blocks = per_sm; }
+    }
+    tune_force(1, -1);
+    if (!rc && items > 0) tune_set(gpu_id, 1, items, best_blocks);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFreeAsync(d_ig, s); cudaFreeAsync(d_corr, s); cudaFreeAsync(d_ph, s);
+    cudaFreeAsync(d_unw, s); cudaFreeAsync(d_cost, s);
+    if (!rc && e != cudaSuccess) rc = cuda_fail(e, "cuphu_autotune");
+    if (!rc && choices) { choices[0] = best_cost; choices[1] = best_blocks; }
+    return rc;
+}
+
 int cuphu_unwrap_ex(const float *igram_c64, const float *corr, const unsigned char *mask,
                     const unsigned char *orig_mask, int nrow, int ncol, CuPhuCostMode cost_mode,
                     const CuPhuParams *params, const CuPhuTileParams *tile,

@@ -531,8 +531,8 @@ __device__ __forceinline__ void store_arc(void *costs, size_t a, const ArcCost &
         reinterpret_cast<short2 *>(costs)[a] = make_short2(o.off, o.sigsq);
 }
 
-template <bool DEFO, int FAM>
-__global__ void __launch_bounds__(256, 3) k_costs7(const float *__restrict__ ph,
+template <bool DEFO, int FAM, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_costs7(const float *__restrict__ ph,
                                                    const float *__restrict__ corr,
                                                    const short *__restrict__ weights, int nrow,
                                                    int ncol, const __grid_constant__ CostConsts k,
@@ -704,18 +704,32 @@ __global__ void __launch_bounds__(256, 3) k_costs7(const float *__restrict__ ph,
     }
 }
 
-template <bool DEFO, int FAM>
-static int launch_costs7_t(const float *ph, const float *corr, const short *weights, int nrow,
+template <bool DEFO, int FAM, int MINB>
+static int launch_costs7_v(const float *ph, const float *corr, const short *weights, int nrow,
                            int ncol, const CostConsts &k, void *costs, cudaStream_t s)
 {
     const int dr = FAM == 0 ? nrow - 1 : nrow, dc = FAM == 0 ? ncol : ncol - 1;
     if (dr < 1 || dc < 1) return 0;
     const int nby = (dr + kC7B - 1) / kC7B, nbx = (dc + kC7B - 1) / kC7B;
     const size_t shm = sizeof(C7Smem);
-    CUPHU_TRY_CUDA(cudaFuncSetAttribute(k_costs7<DEFO, FAM>,
+    CUPHU_TRY_CUDA(cudaFuncSetAttribute(k_costs7<DEFO, FAM, MINB>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-    k_costs7<DEFO, FAM><<<nby * nbx, 256, shm, s>>>(ph, corr, weights, nrow, ncol, k, costs, nbx);
+    k_costs7<DEFO, FAM, MINB><<<nby * nbx, 256, shm, s>>>(ph, corr, weights, nrow, ncol, k, costs,
+                                                          nbx);
     return cuda_fail(cudaGetLastError(), "k_costs7");
+}
+
+/* occupancy variant from the autotuner (default: 3 blocks per SM) */
+template <bool DEFO, int FAM>
+static int launch_costs7_t(const float *ph, const float *corr, const short *weights, int nrow,
+                           int ncol, const CostConsts &k, void *costs, cudaStream_t s)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const long long arcs = 2LL * nrow * ncol;
+    if (tune_get(dev, 0, arcs) == 1)
+        return launch_costs7_v<DEFO, FAM, 4>(ph, corr, weights, nrow, ncol, k, costs, s);
+    return launch_costs7_v<DEFO, FAM, 3>(ph, corr, weights, nrow, ncol, k, costs, s);
 }
 
 /* ── A8 standalone ──────────────────────────────────────────────────────── */

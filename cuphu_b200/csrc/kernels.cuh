@@ -138,6 +138,15 @@ int launch_merge(const ScenePlan *scenes, const ScenePlan *h_scenes, int nscenes
                  const TileDesc *tiles, const SolverPlanes &P, const double *tile_k,
                  const unsigned *comp_off, const SceneOut *sout, cudaStream_t s);
 
+/* tune.cu: kind 0 = cost-kernel variant (0: 3 blocks/SM, 1: 4 blocks/SM),
+ * kind 1 = persistent-solver blocks per SM; -1 = no stored choice */
+int tune_class(long long n);
+int tune_get(int dev, int kind, long long n);
+void tune_set(int dev, int kind, long long n, int v);
+void tune_force(int kind, int v);
+void tune_note_items(long long n);   /* solver job size of the last launch */
+long long tune_probe_items();
+
 /* adjoint.cu */
 int launch_wls_grad(const double *lam, const double *u, const float *gd, const float *gr,
                     const float *wd, const float *wr, int nrow, int ncol, double *ggd, double *ggr,

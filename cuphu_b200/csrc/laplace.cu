@@ -203,7 +203,7 @@ __device__ __forceinline__ ItemXY item_xy(const TileDesc &T, int li)
 /* ── INIT / true residual: b, diag (A10) and r = b - A x, rz partial ────────
  * zero_x: first pass (x = 0, r = b).  write_diag: assemble pass (else the
  * stored diag is reused: residual replacement). */
-template <typename V>
+template <typename V, bool WLS>
 __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, bool zero_x,
                              bool write_diag)
 {
@@ -215,8 +215,9 @@ __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, b
     const float *wd = P.wd + T.pix, *wr = P.wr + T.pix;
     const float *ph = T.ph;
     /* WLS mode: per-arc targets or an explicit right-hand side */
-    const float *gdp = P.gd ? P.gd + T.pix : nullptr, *grp = P.gr ? P.gr + T.pix : nullptr;
-    const float *rhsp = P.rhs ? P.rhs + T.pix : nullptr;
+    const float *gdp = (WLS && P.gd) ? P.gd + T.pix : nullptr;
+    const float *grp = (WLS && P.gr) ? P.gr + T.pix : nullptr;
+    const float *rhsp = (WLS && P.rhs) ? P.rhs + T.pix : nullptr;
     const double eps = (double)kLapEpsF;
     const int r = q.r, nr = T.nr, nc = T.nc, pitch = T.pitch, pp = T.ph_pitch;
     size_t prow = (size_t)r * pitch;
@@ -1032,7 +1033,7 @@ __device__ void run_pass(const SliceCtl &sc, const TileDesc *gt, const TileState
 /* Mixed-precision update pass without shared-memory staging.  The pass is
  * elementwise (r = z diag - alpha q, z = r / diag) plus the r.z dot, so the
  * block sweeps its slice's pixel rows with 16-byte loads straight from HBM
- * (one contiguous row span per plane at a time, not 256-byte item rows), and
+ * (contiguous row spans per plane instead of 256-byte item rows), and
  * each thread accumulates r.z in FP64 over the whole tile segment: one block reduction
  * per tile segment instead of one per item, no barrier per item.  The
  * segment total goes into the partial slot of the segment's first item and
@@ -1060,8 +1061,13 @@ __device__ void run_update_direct(const SliceCtl &sc, const TileDesc *gt, const 
             const int i0 = max(a, band * nbx) - band * nbx, i1 = min(b, (band + 1) * nbx) - band * nbx;
             const int clo = i0 * kItemBx, chi = min(i1 * kItemBx, nc);
             const int rlo = band * kItemBy, rhi = min(rlo + kItemBy, nr);
-            for (int r = rlo; r < rhi; ++r) {
-                for (int c0 = clo + (int)threadIdx.x * kItemVx; c0 < chi; c0 += blockDim.x * kItemVx) {
+            /* the band's (row, 4-column group) pairs spread over all threads,
+             * row-major, so partial bands keep every thread busy */
+            const int qw = (chi - clo + kItemVx - 1) / kItemVx;
+            const int nq = (rhi - rlo) * qw;
+            for (int u = threadIdx.x; u < nq; u += blockDim.x) {
+                {
+                    const int r = rlo + u / qw, c0 = clo + (u - (u / qw) * qw) * kItemVx;
                     const size_t o = (size_t)r * T.pitch + c0;
                     float4 qv = __ldcs(reinterpret_cast<const float4 *>(qp + o));
                     float4 zv = __ldcg(reinterpret_cast<const float4 *>(zp + o));
@@ -1108,7 +1114,10 @@ __device__ __forceinline__ TileState load_state(const TileState *p)
 #define CUPHU_SOLVE_MIN_BLOCKS 3
 #endif
 
-template <typename V>
+/* WLS = true: the WLS-mode instance (explicit arc targets / right-hand
+ * side, optional warm start, no anchoring); a separate instantiation so the
+ * main path's register allocation does not carry its extra inputs */
+template <typename V, bool WLS>
 __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
     k_solve(const TileDesc *__restrict__ tiles, const int *__restrict__ item_tile, int nitems,
             int ntiles, SolverPlanes P, TileState *st, double *part, SolverCtl *ctl,
@@ -1148,8 +1157,8 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
             int a, b;
             slice_items(sc, T, t, a, b);
             for (int li = a; li < b; ++li)
-                store_partial(phase_init<V>(T, li, P, outer == 0 && !sp.warm, true), pbuf[pc & 1],
-                              T.item0 + li, sw);
+                store_partial(phase_init<V, WLS>(T, li, P, outer == 0 && !(WLS && sp.warm), true),
+                              pbuf[pc & 1], T.item0 + li, sw);
             if (b > a) seg_done(T, t, b - a, pbuf[pc & 1], tbuf[pc & 1], tick, sw, &s_bcast, &s_flag);
         }
         ++pc;
@@ -1275,7 +1284,7 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
                     if (sc.pre[t + 1] == sc.pre[t]) continue;
                     slice_items(sc, T, t, a, b);
                     for (int li = a; li < b; ++li)
-                        store_partial(phase_init<V>(T, li, P, false, false), pbuf[pc & 1],
+                        store_partial(phase_init<V, WLS>(T, li, P, false, false), pbuf[pc & 1],
                                       T.item0 + li, sw);
                     if (b > a)
                         seg_done(T, t, b - a, pbuf[pc & 1], tbuf[pc & 1], tick, sw, &s_bcast,
@@ -1323,7 +1332,7 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
             if (!grid_sync(ctl, timeout_ns)) return;
         }
     }
-    if (sp.wls) return;   /* WLS mode: the caller reads the raw solution x */
+    if (WLS) return;   /* WLS mode: the caller reads the raw solution x */
     setup_slice(sc, tiles, nullptr, ntiles, sw);
     for (int t = sc.t0; t <= sc.t1; ++t) {
         const TileDesc &T = stile(sc, tiles, t);
@@ -1389,8 +1398,8 @@ static int make_maps(SolveMaps &M, const SolverPlanes &P, int pitch, int rows)
     return rc ? CUPHU_ERR_CUDA : 0;
 }
 
-template <typename V>
-static int launch_solve_t(const TileDesc *tiles, const int *item_tile, int nitems, int ntiles,
+template <typename V, bool WLS>
+static int launch_solve_kernel(const TileDesc *tiles, const int *item_tile, int nitems, int ntiles,
                           const SolverPlanes &P, int pitch, int rows, TileState *st, double *part,
                           SolverCtl *ctl, const SolveParams &sp, long long timeout_ns, int device,
                           cudaStream_t s)
@@ -1403,11 +1412,15 @@ static int launch_solve_t(const TileDesc *tiles, const int *item_tile, int nitem
     int nsm = 0, per_sm = 0;
     CUPHU_TRY_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
     const size_t smem = solve_smem_bytes<V>();
-    CUPHU_TRY_CUDA(cudaFuncSetAttribute(k_solve<V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CUPHU_TRY_CUDA(cudaFuncSetAttribute(k_solve<V, WLS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)smem));
-    CUPHU_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve<V>,
+    CUPHU_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve<V, WLS>,
                                                                  kItemThreads, smem));
     if (per_sm < 1) return fail(CUPHU_ERR_CUDA, "solver kernel cannot be resident");
+    /* blocks per SM from the autotuner (job size = item count) */
+    tune_note_items(nitems);
+    const int tuned = tune_get(device, 1, (long long)nitems);
+    if (tuned >= 1) per_sm = std::min(per_sm, tuned);
     int grid = std::min(nsm * per_sm, std::max(nitems, 1));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
@@ -1419,9 +1432,22 @@ static int launch_solve_t(const TileDesc *tiles, const int *item_tile, int nitem
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    CUPHU_TRY_CUDA(cudaLaunchKernelEx(&cfg, k_solve<V>, tiles, item_tile, nitems, ntiles, P, st,
+    CUPHU_TRY_CUDA(cudaLaunchKernelEx(&cfg, k_solve<V, WLS>, tiles, item_tile, nitems, ntiles, P, st,
                                       part, ctl, sp, timeout_ns, M));
     return 0;
+}
+
+template <typename V>
+static int launch_solve_t(const TileDesc *tiles, const int *item_tile, int nitems, int ntiles,
+                          const SolverPlanes &P, int pitch, int rows, TileState *st, double *part,
+                          SolverCtl *ctl, const SolveParams &sp, long long timeout_ns, int device,
+                          cudaStream_t s)
+{
+    if (sp.wls)
+        return launch_solve_kernel<V, true>(tiles, item_tile, nitems, ntiles, P, pitch, rows, st,
+                                            part, ctl, sp, timeout_ns, device, s);
+    return launch_solve_kernel<V, false>(tiles, item_tile, nitems, ntiles, P, pitch, rows, st, part,
+                                         ctl, sp, timeout_ns, device, s);
 }
 
 int launch_solve(bool fp64, const TileDesc *tiles, const int *item_tile, int nitems,

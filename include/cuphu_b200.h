@@ -257,6 +257,20 @@ int cuphu_laplace_solve_device(const void *d_costs, int cost_stride_shorts,
                                int32_t *d_cycles, float *d_cont, CuPhuSolveStats *stats,
                                void *stream);
 
+/* ── launch-shape autotuner (new) ─────────────────────────────────────────
+ * Times, on the caller's scene (host pointers, uploaded here), the cost
+ * kernel at 3 and 4 blocks per SM and the persistent solver at 2 and 3
+ * blocks per SM (a 20-iteration probe with the given tiling), and stores the
+ * faster choice per device and job-size class (floor(log2) of the arc or
+ * work-item count) for all later calls.  choices (optional, int[2]) receives
+ * {cost variant 0|1, solver blocks per SM}.  Costs and FP64 solves are
+ * identical for every choice; mixed-precision update passes reduce in the
+ * grid's segmentation, so a mixed solve is deterministic per choice.
+ * CUPHU_TUNE=0 in the environment ignores stored choices. */
+int cuphu_autotune(const float *igram_c64, const float *corr, int nrow, int ncol,
+                   CuPhuCostMode cost_mode, const CuPhuParams *params,
+                   const CuPhuTileParams *tile, int gpu_id, int *choices);
+
 /* ── batched pipeline as a CUDA graph (new) ─────────────────────────────────
  * Plans the batch once into a workspace owned by the graph object, uploads
  * its descriptors and captures the whole device pipeline (state resets,

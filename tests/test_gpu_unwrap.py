@@ -139,6 +139,24 @@ def test_batch_graph_replays_the_batch(torch_cuda):
         check(lib().cuphu_batch_graph_destroy(graph))
 
 
+def test_autotune_keeps_results(torch_cuda):
+    """After cuphu_autotune stores its choices for this size, costs stay bit
+    exact and the FP64 pipeline stays bit exact with the oracle."""
+    import cuphu_b200
+    ig, g, _, _ = S.bumps(200, 260, seed=61, nbumps=3, amp_range=(5, 20), sigma_range=(8, 30))
+    ph = O.phase_from_igram(ig)
+    base_u, base_c, _ = device_unwrap(torch_cuda, ph, g, 5.0, (2, 2), (16, 16), precision=1,
+                                      n_irls=2)
+    ch = cuphu_b200.autotune(ig, g, 5.0, cost="defo", ntiles=(2, 2), tile_overlap=(16, 16))
+    assert ch["cost_blocks_per_sm"] in (3, 4) and ch["solver_blocks_per_sm"] in (2, 3)
+    u, c, _ = device_unwrap(torch_cuda, ph, g, 5.0, (2, 2), (16, 16), precision=1, n_irls=2)
+    assert np.array_equal(u.view(np.int32), base_u.view(np.int32))
+    assert np.array_equal(c, base_c)
+    from tests.test_gpu_kernels import gpu_costs
+    got = gpu_costs(torch_cuda, ph, g, 5.0, 1)
+    assert np.array_equal(got, O.build_costs(ph, g, 5.0, mode=1))
+
+
 def test_reference_pixel_shift_and_cc_on_device(torch_cuda):
     ig, g, _, _ = S.bumps(90, 110, seed=8, nbumps=2, amp_range=(10, 30), sigma_range=(10, 30))
     ph = O.phase_from_igram(ig)
