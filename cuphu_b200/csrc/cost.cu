@@ -401,7 +401,15 @@ struct C7Smem {
     C7Deferred q[kC7Q];
     short lay[kC7Tab];
     int qn;
+    unsigned gbase;
 };
+/* launch-wide queue of deferred arcs, finished by k_costs7_drain */
+struct C7Global {
+    float ca, cb, dp, av;
+    unsigned long long a;
+    int w, pad;
+};
+constexpr unsigned kC7NoSlot = 0xffffffffu;
 
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 /* a - b per lane, one rounding */
@@ -536,7 +544,9 @@ __global__ void __launch_bounds__(256, MINB) k_costs7(const float *__restrict__ 
                                                    const float *__restrict__ corr,
                                                    const short *__restrict__ weights, int nrow,
                                                    int ncol, const __grid_constant__ CostConsts k,
-                                                   void *__restrict__ costs_out, int nbx)
+                                                   void *__restrict__ costs_out, int nbx,
+                                                   C7Global *__restrict__ gq, unsigned *gqn,
+                                                   unsigned gqcap)
 {
     extern __shared__ __align__(16) char c7raw[];
     C7Smem &S = *reinterpret_cast<C7Smem *>(c7raw);
@@ -693,20 +703,47 @@ __global__ void __launch_bounds__(256, MINB) k_costs7(const float *__restrict__ 
     }
     }
     __syncthreads();
-    /* deferred arcs: the reference's FP64 arithmetic, all lanes busy */
+    /* deferred arcs: handed to the launch-wide queue (finished by
+     * k_costs7_drain with full warps) when it has room, else the
+     * reference's FP64 arithmetic here */
     const int nq = min(S.qn, kC7Q);
+    if (tid == 0) S.gbase = (gq && nq > 0) ? atomicAdd(gqn, (unsigned)nq) : kC7NoSlot;
+    __syncthreads();
+    /* slots below the capacity are the queue's; a block that reaches past
+     * it finishes the rest itself, so the first min(count, capacity) slots
+     * are always valid */
+    const unsigned gb = S.gbase;
     for (int i = tid; i < nq; i += blockDim.x) {
         const C7Deferred e = S.q[i];
         const int ar = r0 + e.rc / kC7B, ac = c0 + e.rc % kC7B;
         const size_t a = FAM == 0 ? (size_t)ar * ncol + ac : nra + (size_t)ar * (ncol - 1) + ac;
-        store_arc<DEFO>(costs_out, a,
+        if (gb != kC7NoSlot && gb < gqcap && (unsigned)i < gqcap - gb)
+            gq[gb + i] = C7Global{e.ca, e.cb, e.dp, e.av, (unsigned long long)a, e.w, 0};
+        else
+            store_arc<DEFO>(costs_out, a,
+                            arc_cost<DEFO>((double)e.ca, (double)e.cb, e.dp, e.av, (short)e.w, k));
+    }
+}
+
+template <bool DEFO>
+__global__ void __launch_bounds__(256) k_costs7_drain(const C7Global *__restrict__ gq,
+                                                      const unsigned *__restrict__ gqn,
+                                                      unsigned gqcap,
+                                                      const __grid_constant__ CostConsts k,
+                                                      void *__restrict__ costs_out)
+{
+    const unsigned n = min(*gqn, gqcap);
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const C7Global e = gq[i];
+        store_arc<DEFO>(costs_out, (size_t)e.a,
                         arc_cost<DEFO>((double)e.ca, (double)e.cb, e.dp, e.av, (short)e.w, k));
     }
 }
 
 template <bool DEFO, int FAM, int MINB>
 static int launch_costs7_v(const float *ph, const float *corr, const short *weights, int nrow,
-                           int ncol, const CostConsts &k, void *costs, cudaStream_t s)
+                           int ncol, const CostConsts &k, void *costs, C7Global *gq,
+                           unsigned *gqn, unsigned gqcap, cudaStream_t s)
 {
     const int dr = FAM == 0 ? nrow - 1 : nrow, dc = FAM == 0 ? ncol : ncol - 1;
     if (dr < 1 || dc < 1) return 0;
@@ -715,21 +752,54 @@ static int launch_costs7_v(const float *ph, const float *corr, const short *weig
     CUPHU_TRY_CUDA(cudaFuncSetAttribute(k_costs7<DEFO, FAM, MINB>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
     k_costs7<DEFO, FAM, MINB><<<nby * nbx, 256, shm, s>>>(ph, corr, weights, nrow, ncol, k, costs,
-                                                          nbx);
+                                                          nbx, gq, gqn, gqcap);
     return cuda_fail(cudaGetLastError(), "k_costs7");
 }
 
 /* occupancy variant from the autotuner (default: 3 blocks per SM) */
 template <bool DEFO, int FAM>
 static int launch_costs7_t(const float *ph, const float *corr, const short *weights, int nrow,
-                           int ncol, const CostConsts &k, void *costs, cudaStream_t s)
+                           int ncol, const CostConsts &k, void *costs, C7Global *gq,
+                           unsigned *gqn, unsigned gqcap, cudaStream_t s)
 {
     int dev = 0;
     cudaGetDevice(&dev);
     const long long arcs = 2LL * nrow * ncol;
     if (tune_get(dev, 0, arcs) == 1)
-        return launch_costs7_v<DEFO, FAM, 4>(ph, corr, weights, nrow, ncol, k, costs, s);
-    return launch_costs7_v<DEFO, FAM, 3>(ph, corr, weights, nrow, ncol, k, costs, s);
+        return launch_costs7_v<DEFO, FAM, 4>(ph, corr, weights, nrow, ncol, k, costs, gq, gqn,
+                                             gqcap, s);
+    return launch_costs7_v<DEFO, FAM, 3>(ph, corr, weights, nrow, ncol, k, costs, gq, gqn, gqcap,
+                                         s);
+}
+
+/* both arc families, then the queued arcs; the queue (about one arc in 128
+ * of room) is stream-ordered scratch, and blocks that find it full finish
+ * their deferred arcs themselves */
+template <bool DEFO>
+static int launch_costs7_all(const float *ph, const float *corr, const short *weights, int nrow,
+                             int ncol, const CostConsts &k, void *costs, cudaStream_t s)
+{
+    const unsigned long long narcs =
+        (unsigned long long)(nrow - 1) * ncol + (unsigned long long)nrow * (ncol - 1);
+    const unsigned cap = (unsigned)std::min<unsigned long long>(narcs / 128 + 4096, 1u << 24);
+    void *buf = nullptr;
+    C7Global *gq = nullptr;
+    unsigned *gqn = nullptr;
+    if (cudaMallocAsync(&buf, (size_t)cap * sizeof(C7Global) + 256, s) == cudaSuccess) {
+        gqn = reinterpret_cast<unsigned *>(buf);
+        gq = reinterpret_cast<C7Global *>(static_cast<char *>(buf) + 256);
+        CUPHU_TRY_CUDA(cudaMemsetAsync(gqn, 0, sizeof(unsigned), s));
+    } else {
+        cudaGetLastError();
+    }
+    int rc = launch_costs7_t<DEFO, 0>(ph, corr, weights, nrow, ncol, k, costs, gq, gqn, cap, s);
+    if (!rc) rc = launch_costs7_t<DEFO, 1>(ph, corr, weights, nrow, ncol, k, costs, gq, gqn, cap, s);
+    if (!rc && gq) {
+        k_costs7_drain<DEFO><<<148 * 4, 256, 0, s>>>(gq, gqn, cap, k, costs);
+        rc = cuda_fail(cudaGetLastError(), "k_costs7_drain");
+    }
+    if (buf) cudaFreeAsync(buf, s);
+    return rc;
 }
 
 /* ── A8 standalone ──────────────────────────────────────────────────────── */
@@ -876,12 +946,8 @@ int launch_costs(const float *ph, const float *corr, const short *weights, int n
     const bool w7 = kperp / 2 == 3 && kpar / 2 == 3;
     if (w7) {
         int rc = mode == CUPHU_COST_SMOOTH
-                     ? launch_costs7_t<false, 0>(ph, corr, weights, nrow, ncol, k, costs, s)
-                     : launch_costs7_t<true, 0>(ph, corr, weights, nrow, ncol, k, costs, s);
-        if (!rc)
-            rc = mode == CUPHU_COST_SMOOTH
-                     ? launch_costs7_t<false, 1>(ph, corr, weights, nrow, ncol, k, costs, s)
-                     : launch_costs7_t<true, 1>(ph, corr, weights, nrow, ncol, k, costs, s);
+                     ? launch_costs7_all<false>(ph, corr, weights, nrow, ncol, k, costs, s)
+                     : launch_costs7_all<true>(ph, corr, weights, nrow, ncol, k, costs, s);
         if (!rc && res) rc = launch_residues(ph, nrow, ncol, res, s);
         return rc;
     }
