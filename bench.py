@@ -42,8 +42,8 @@ METRIC = "Mpix/s unwrapped at 8192^2 (mixed-precision Laplace PCG)"
 
 
 # measured k_solve DRAM bytes (mixed precision), see the roofline block
-TRAFFIC_PER_PX_ITER = 50.1
-TRAFFIC_PER_PASS_PX = 71.0
+TRAFFIC_PER_PX_ITER = 50.3
+TRAFFIC_PER_PASS_PX = 65.0
 
 
 def hbm_peak():
