@@ -166,10 +166,12 @@ __device__ __forceinline__ float div_7(float x)
  * the result is bit-identical to the reference arithmetic. */
 /* the reference's FP64 arithmetic (cuphu_cost.cu:109-117); out of line, the
  * screen above sends it about one arc in a hundred */
-__device__ __noinline__ int trunc_sigsq_exact(double b, short w, const CostConsts &k)
+__device__ __noinline__ int trunc_sigsq_exact(double b, short w, double sigsqrhoconst,
+                                              double rhopow, double sigsqcorr, double nsc2,
+                                              double costscale)
 {
-    double sigsqrho = __dmul_rn(__fma_rn(k.sigsqrhoconst, pow(b, k.rhopow), k.sigsqcorr), k.nsc2);
-    return (int)(sigsqrho / (k.costscale * (double)w));
+    double sigsqrho = __dmul_rn(__fma_rn(sigsqrhoconst, pow(b, rhopow), sigsqcorr), nsc2);
+    return (int)(sigsqrho / (costscale * (double)w));
 }
 
 __device__ __forceinline__ int trunc_sigsq(double rho, short w, const CostConsts &k)
@@ -187,7 +189,9 @@ __device__ __forceinline__ int trunc_sigsq(double rho, short w, const CostConsts
         float lo = floorf(v - m);
         if (lo == floorf(v + m) && lo >= 0.0f && v + m < 1.0e7f) return (int)lo;
     }
-    return trunc_sigsq_exact(b, w, k);
+    /* scalars by value: the constants' struct is never address-taken, so the
+     * kernels read it from the parameter bank directly */
+    return trunc_sigsq_exact(b, w, k.sigsqrhoconst, k.rhopow, k.sigsqcorr, k.nsc2, k.costscale);
 }
 
 __device__ __forceinline__ int sigsq_of(double ca, double cb, short w, const CostConsts &k)
@@ -543,7 +547,7 @@ template <bool DEFO, int FAM, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_costs7(const float *__restrict__ ph,
                                                    const float *__restrict__ corr,
                                                    const short *__restrict__ weights, int nrow,
-                                                   int ncol, const __grid_constant__ CostConsts k,
+                                                   int ncol, const CostConsts k,
                                                    void *__restrict__ costs_out, int nbx,
                                                    C7Global *__restrict__ gq, unsigned *gqn,
                                                    unsigned gqcap)
@@ -728,8 +732,7 @@ __global__ void __launch_bounds__(256, MINB) k_costs7(const float *__restrict__ 
 template <bool DEFO>
 __global__ void __launch_bounds__(256) k_costs7_drain(const C7Global *__restrict__ gq,
                                                       const unsigned *__restrict__ gqn,
-                                                      unsigned gqcap,
-                                                      const __grid_constant__ CostConsts k,
+                                                      unsigned gqcap, const CostConsts k,
                                                       void *__restrict__ costs_out)
 {
     const unsigned n = min(*gqn, gqcap);
