@@ -34,7 +34,6 @@
 
 namespace cuphu {
 
-constexpr int kHaloW = kItemBx + 2;
 constexpr int kHaloH = kItemBy + 2;
 
 /* ── vector access helpers (L2-coherent loads of in-kernel-written data) ── */

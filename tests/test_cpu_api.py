@@ -50,7 +50,8 @@ def test_defaults_and_no_gpu_queries():
     assert (t.ntilerow, t.ntilecol, t.tilecostthresh, t.minregionsize) == (1, 1, 500, 100)
 
 
-REF_H = "/root/reference/src/cxx/cuphu/cuphu.h"
+REF_H = os.path.join(os.environ.get("CUPHU_REFERENCE_ROOT", "/root/reference"),
+                     "src/cxx/cuphu/cuphu.h")
 
 
 @pytest.mark.skipif(not os.path.exists(REF_H), reason="reference header not present")
