@@ -151,3 +151,36 @@ def test_status_errors_on_cpu():
                         C.byref(p), C.byref(t), None, None, 0, C.byref(res))
     assert rc == -3
     assert L.cuphu_last_error()
+
+
+def test_new_entry_points_validate_before_touching_cuda():
+    """WLS solve/gradient, batch graph and autotuner reject bad arguments
+    with CUPHU_ERR_INVALID before any CUDA call (runs without a GPU)."""
+    L = _lib.lib()
+    o = _lib.default_solve_options()
+    p = _lib.default_params()
+    t = _lib.default_tile_params()
+    a = np.ones(16, np.float32)
+    pa = _lib.ptr(a)
+    u = np.zeros(16, np.float64)
+    pu = _lib.ptr(u)
+    # both targets and a right-hand side
+    assert L.cuphu_wls_solve_device(pa, pa, pa, pa, pa, None, 4, 4, C.byref(o), pu, None,
+                                    None) == -2
+    assert b"either" in L.cuphu_last_error()
+    # only one of the two target planes
+    assert L.cuphu_wls_solve_device(pa, None, None, pa, pa, None, 4, 4, C.byref(o), pu, None,
+                                    None) == -2
+    # missing weights / output / empty shape
+    assert L.cuphu_wls_solve_device(pa, pa, None, None, pa, None, 4, 4, C.byref(o), pu, None,
+                                    None) == -2
+    assert L.cuphu_wls_solve_device(pa, pa, None, pa, pa, None, 0, 4, C.byref(o), pu, None,
+                                    None) == -2
+    assert L.cuphu_wls_grad_device(pu, pu, pa, pa, pa, pa, 4, 4, pu, pu, pu, None, None) == -2
+    graph = C.c_void_p()
+    assert L.cuphu_batch_graph_create(None, 0, 0, C.byref(p), C.byref(o), C.byref(graph)) == -2
+    assert L.cuphu_batch_graph_create(None, 1, 0, C.byref(p), C.byref(o), None) == -2
+    assert L.cuphu_batch_graph_launch(None, None) == -2
+    assert L.cuphu_batch_graph_destroy(None) == 0
+    assert L.cuphu_autotune(pa, pa, 1, 4, 0, C.byref(p), C.byref(t), 0, None) == -2
+    assert L.cuphu_autotune(pa, pa, 4, 4, 7, C.byref(p), C.byref(t), 0, None) == -2
