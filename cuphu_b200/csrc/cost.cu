@@ -21,7 +21,11 @@
 #include "common.cuh"
 #include "kernels.cuh"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <cmath>
+#include <cstring>
 
 namespace cuphu {
 
@@ -399,14 +403,55 @@ struct C7Deferred {
     float ca, cb, dp, av;
     int rc, w;
 };
+/* TMA staging (when the planes allow it): the phase window as one box of
+ * columns c0-4 .. c0+71 (x 16-byte aligned) and rows r0-3 .. r0+67, and the
+ * coherence window of columns c0 .. c0+67, rows r0 .. r0+64 */
+constexpr int kC7WinW = 76, kC7WinH = 71;
+constexpr int kC7CorW = 68, kC7CorH = 65;
 struct C7Smem {
-    float2 php[(kC7W + 1) * kC7PP];   /* phase pairs, then the row sums */
-    float2 dpp[kC7W * kC7PP];         /* difference pairs */
+    union {
+        float2 php[(kC7W + 1) * kC7PP];   /* phase pairs (load path), then the row sums */
+        float win[kC7WinH * kC7WinW];     /* phase window (TMA path) */
+    };
+    float2 dpp[kC7W * kC7PP];             /* difference pairs */
+    alignas(128) float cor[kC7CorH * kC7CorW];   /* coherence window (TMA path) */
     C7Deferred q[kC7Q];
     short lay[kC7Tab];
+    unsigned long long bar;
     int qn;
     unsigned gbase;
 };
+static_assert(sizeof(float) * kC7WinH * kC7WinW <= sizeof(float2) * (kC7W + 1) * kC7PP,
+              "phase window must fit the pair buffer");
+static_assert(kC7WinW * 4 % 16 == 0 && kC7CorW * 4 % 16 == 0, "TMA boxes: 16-byte rows");
+
+__device__ __forceinline__ unsigned c7_smem(const void *p)
+{
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void c7_tma_2d(void *dst, const CUtensorMap *map, int x, int y,
+                                          unsigned long long *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];" ::"r"(c7_smem(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(c7_smem(bar))
+        : "memory");
+}
+/* bounded wait for the block's TMA boxes (parity 0: one use per block) */
+__device__ __forceinline__ void c7_wait(unsigned long long *bar)
+{
+    for (int i = 0; i < (1 << 24); ++i) {
+        unsigned ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
+            " selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(ok)
+            : "r"(c7_smem(bar))
+            : "memory");
+        if (ok) return;
+    }
+}
 /* launch-wide queue of deferred arcs, finished by k_costs7_drain */
 struct C7Global {
     float ca, cb, dp, av;
@@ -550,10 +595,13 @@ __global__ void __launch_bounds__(256, MINB) k_costs7(const float *__restrict__ 
                                                    int ncol, const CostConsts k,
                                                    void *__restrict__ costs_out, int nbx,
                                                    C7Global *__restrict__ gq, unsigned *gqn,
-                                                   unsigned gqcap)
+                                                   unsigned gqcap, int tma,
+                                                   const __grid_constant__ CUtensorMap tm_ph,
+                                                   const __grid_constant__ CUtensorMap tm_cor)
 {
     extern __shared__ __align__(16) char c7raw[];
-    C7Smem &S = *reinterpret_cast<C7Smem *>(c7raw);
+    C7Smem &S = *reinterpret_cast<C7Smem *>(
+        ((uintptr_t)c7raw + 127) & ~(uintptr_t)127);
     const int by = blockIdx.x / nbx, bx = blockIdx.x - (blockIdx.x / nbx) * nbx;
     const int dr = FAM == 0 ? nrow - 1 : nrow;
     const int dc = FAM == 0 ? ncol : ncol - 1;
@@ -570,7 +618,34 @@ __global__ void __launch_bounds__(256, MINB) k_costs7(const float *__restrict__ 
     constexpr int NP = kC7W - kC7H + (FAM == 1 ? 1 : 0);      /* phase pairs per row */
     constexpr int ND = kC7W - kC7H;                            /* difference pairs per row */
     const bool interior = r0 >= 3 && r0 + kC7B + 3 <= dr && c0 >= 3 && c0 + kC7B + 3 <= dc;
-    if (interior) {
+    if (tma) {
+        if (tid == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(c7_smem(&S.bar))
+                         : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            const unsigned tx = (unsigned)(kC7CorH * kC7CorW * 4) +
+                                (interior ? (unsigned)(kC7WinH * kC7WinW * 4) : 0u);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                             c7_smem(&S.bar)),
+                         "r"(tx)
+                         : "memory");
+            c7_tma_2d(S.cor, &tm_cor, c0, r0, &S.bar);
+            if (interior) c7_tma_2d(S.win, &tm_ph, c0 - 4, r0 - 3, &S.bar);
+        }
+        __syncthreads();
+        c7_wait(&S.bar);
+    }
+    if (interior && tma) {
+        /* differences from the row-major window (column c0-3+j is win[.][j+1]) */
+        for (int u = tid; u < kC7W * ND; u += blockDim.x) {
+            const int i = u / ND, j = u - (u / ND) * ND;
+            const float *w0 = S.win + i * kC7WinW + j + 1;
+            const float2 x = FAM == 0
+                                 ? sub2(f2(w0[0], w0[kC7H]), f2(w0[kC7WinW], w0[kC7WinW + kC7H]))
+                                 : sub2(f2(w0[1], w0[kC7H + 1]), f2(w0[0], w0[kC7H]));
+            S.dpp[i * kC7PP + j] = wrap2(div_2pi2(x));
+        }
+    } else if (interior) {
         /* all of a thread's window loads in flight before the first store */
         const float *src = ph + (size_t)(r0 - 3) * ncol + (c0 - 3);
         constexpr int NU = (NR * NP + 255) / 256;
@@ -656,7 +731,12 @@ __global__ void __launch_bounds__(256, MINB) k_costs7(const float *__restrict__ 
             const int rr = r0 + rs + q;
             cv[h][q] = 0.0f;
             if (q < 4) cw[h][q] = 0.0f;
-            if (FAM == 0) {
+            if (tma) {
+                /* staged window: row rs+q, column j+32h (+1); zero outside the array */
+                const float *cp = S.cor + (rs + q) * kC7CorW + j + h * kC7H;
+                if (FAM == 0) cv[h][q] = cp[0];
+                else if (q < 4) { cv[h][q] = cp[0]; cw[h][q] = cp[1]; }
+            } else if (FAM == 0) {
                 if (ac < dc && rr < nrow) cv[h][q] = __ldg(corr + (size_t)rr * ncol + ac);
             } else if (q < 4 && ac < dc && rr < nrow) {
                 cv[h][q] = __ldg(corr + (size_t)rr * ncol + ac);
@@ -743,6 +823,39 @@ __global__ void __launch_bounds__(256) k_costs7_drain(const C7Global *__restrict
     }
 }
 
+static PFN_cuTensorMapEncodeTiled_v12000 c7_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+/* TMA map of an nrow x ncol float plane with the given box; false when the
+ * plane's base or row pitch is not 16-byte aligned (the load path is used) */
+static bool c7_map(CUtensorMap &m, const float *base, int nrow, int ncol, int bx, int by)
+{
+    if (((uintptr_t)base & 15) || (ncol & 3)) return false;
+    auto enc = c7_encoder();
+    if (!enc) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)ncol, (cuuint64_t)nrow};
+    cuuint64_t strides[1] = {(cuuint64_t)ncol * 4};
+    cuuint32_t box[2] = {(cuuint32_t)bx, (cuuint32_t)by};
+    cuuint32_t es[2] = {1, 1};
+    return enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(base), dims, strides,
+               box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <bool DEFO, int FAM, int MINB>
 static int launch_costs7_v(const float *ph, const float *corr, const short *weights, int nrow,
                            int ncol, const CostConsts &k, void *costs, C7Global *gq,
@@ -751,11 +864,17 @@ static int launch_costs7_v(const float *ph, const float *corr, const short *weig
     const int dr = FAM == 0 ? nrow - 1 : nrow, dc = FAM == 0 ? ncol : ncol - 1;
     if (dr < 1 || dc < 1) return 0;
     const int nby = (dr + kC7B - 1) / kC7B, nbx = (dc + kC7B - 1) / kC7B;
-    const size_t shm = sizeof(C7Smem);
+    const size_t shm = sizeof(C7Smem) + 128;
+    CUtensorMap tm_ph, tm_cor;
+    std::memset(&tm_ph, 0, sizeof(tm_ph));
+    std::memset(&tm_cor, 0, sizeof(tm_cor));
+    const int tma = (c7_map(tm_ph, ph, nrow, ncol, kC7WinW, kC7WinH) &&
+                     c7_map(tm_cor, corr, nrow, ncol, kC7CorW, kC7CorH)) ? 1 : 0;
     CUPHU_TRY_CUDA(cudaFuncSetAttribute(k_costs7<DEFO, FAM, MINB>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
     k_costs7<DEFO, FAM, MINB><<<nby * nbx, 256, shm, s>>>(ph, corr, weights, nrow, ncol, k, costs,
-                                                          nbx, gq, gqn, gqcap);
+                                                          nbx, gq, gqn, gqcap, tma, tm_ph,
+                                                          tm_cor);
     return cuda_fail(cudaGetLastError(), "k_costs7");
 }
 
