@@ -57,7 +57,7 @@ CostConsts make_cost_consts(const CuPhuParams &p)
     k.dzmax = std::max(1, std::min(dzi, 32767));
 
     /* FP32 fast path (k_costs7): every quantity it rounds is bracketed by a
-     * margin above its FP32 error bound; see arc_fast */
+     * margin above its FP32 error bound; see arc_fast2 */
     k.fast = 0;
     k.nsc_f = (float)k.nsc;
     k.thr_lo = std::nextafter((float)(k.thresh * (1.0 - std::ldexp(1.0, -20))), 0.0f);
@@ -386,10 +386,11 @@ __global__ void __launch_bounds__(256) k_costs(const float *__restrict__ ph,
  *    division by 2 pi, re-wrap, 7-term sums, division by 7 -- runs as paired
  *    FP32 instructions (__fadd2_rn, __ffma2_rn, __fmul2_rn: IEEE
  *    round-to-nearest per lane, the reference's per-element arithmetic);
- *  - the per-arc cost is evaluated in FP32 with error margins (arc_fast);
+ *  - the per-arc cost is evaluated in FP32 with error margins (arc_fast2);
  *    the few arcs whose integer results a margin cannot decide are queued in
- *    shared memory and finished by arc_cost's FP64 reference arithmetic
- *    after the strip loop, by all threads of the block together.
+ *    shared memory, then in a launch-wide queue that k_costs7_drain
+ *    finishes with arc_cost's FP64 reference arithmetic (a block whose
+ *    arcs do not fit the queue finishes them itself).
  * Summation order and rounding of the box-car follow cuphu_util.cu:104-181:
  * s = 0, s += d[k] for k = 0..6, then s / 7. */
 constexpr int kC7B = 64;        /* arcs per block edge */
@@ -512,8 +513,8 @@ __device__ __forceinline__ float ex2_ftz(float x)
     return y;
 }
 
-/* FP32 evaluation of arc_cost for weight 1 and coherences in [0, 1].  Each
- * rounded decision is taken only when the FP32 value is farther from the
+/* arc_lane / arc_fast2: FP32 evaluation of arc_cost for weight 1 and
+ * coherences in [0, 1].  Each rounded decision is taken only when the FP32 value is farther from the
  * decision boundary than the bound on its distance to the reference's FP64
  * value, so the integers equal the reference's; otherwise returns false.
  *  rho:    rho_f = RN(ca + cb)/2 is within 2^-23 relative of the reference's
@@ -527,48 +528,33 @@ __device__ __forceinline__ float ex2_ftz(float x)
  *          b^rhopow and the FMA stay within 2e-6 rhopow + 5e-7 relative, and
  *          the screen (1e-5 (1 + rhopow) + 2e-6 relative + 1e-6) brackets the
  *          truncation point with at least a 5x margin.
- *  rho = 0 uses the exact host value of the reference's formula at b = 1. */
+ *  rho = 0 uses the exact host value of the reference's formula at b = 1.
+ * arc_lane takes one lane's decisions from the values arc_fast2 computed. */
 template <bool DEFO>
-__device__ __forceinline__ bool arc_fast(float ca, float cb, float dp, float av,
+__device__ __forceinline__ bool arc_lane(float ca, float cb, float rho, float X, float XM, float f,
+                                         float b, float v, float vm, float fr, float m,
                                          const CostConsts &k, const short *lay, int ntab,
                                          ArcCost &o)
 {
-    if (!(ca >= 0.0f && ca <= 1.0f && cb >= 0.0f && cb <= 1.0f)) return false;
-    const float rho = 0.5f * __fadd_rn(ca, cb);
+    bool ok = (ca >= 0.0f) & (ca <= 1.0f) & (cb >= 0.0f) & (cb <= 1.0f);
     const bool pos = rho >= k.thr_hi;
-    if (!pos && !(rho <= k.thr_lo)) return false;
-    const float sel = pos ? av : 0.5f * av;
-    const float X = __fmul_rn(__fsub_rn(dp, sel), k.nsc_f);
-    const float XM = __fadd_rn(X, 12582912.0f);
+    ok &= pos | (rho <= k.thr_lo);
     int off_i = __float_as_int(XM) - 0x4B400000;
-    const float f = __fsub_rn(X, __fsub_rn(XM, 12582912.0f));
     if (DEFO) {
-        if (fabsf(f) > 0.5f - k.m_off) return false;
+        ok &= fabsf(f) <= 0.5f - k.m_off;
     } else {
-        if (fabsf(f) < k.m_off) return false;
+        ok &= fabsf(f) >= k.m_off;
         off_i += (f > 0.0f && X < 0.0f) ? 1 : 0;
         off_i -= (f < 0.0f && X > 0.0f) ? 1 : 0;
     }
-    int sg;
-    if (pos) {
-        const float b = 0.5f * __fadd_rn(1.0f - ca, 1.0f - cb);
-        if (!(b >= 0x1p-8f && b <= 1.0f)) return false;
-        const float pw = ex2_ftz(__fmul_rn(k.rhopow_f, lg2_ftz(b)));
-        const float v = __fmaf_rn(k.a_f, pw, k.c_f);
-        if (!(v >= 0.0f && v < 1.0e6f)) return false;
-        const float vm = __fadd_rn(__fsub_rn(v, 0.5f), 12582912.0f);
-        sg = __float_as_int(vm) - 0x4B400000;
-        const float fr = __fsub_rn(v, __fsub_rn(vm, 12582912.0f));
-        const float m = __fmaf_rn(k.screen_f, v, 1e-6f);
-        if (fr < m || fr > 1.0f - m) return false;
-    } else {
-        sg = k.s_rho0;
-    }
-    sg = max(sg, k.sigsqshortmin);
+    const bool okp = (b >= 0x1p-8f) & (b <= 1.0f) & (v >= 0.0f) & (v < 1.0e6f) & (fr >= m) &
+                     (fr <= 1.0f - m);
+    ok &= !pos | okp;
+    const int sg = max(pos ? __float_as_int(vm) - 0x4B400000 : k.s_rho0, k.sigsqshortmin);
     if (DEFO) {
-        if (sg >= ntab) return false;
+        ok &= sg < ntab;
         o.dzmax = (short)k.dzmax;
-        o.laycost = lay[sg];
+        o.laycost = lay[min(max(sg, 0), ntab - 1)];
     } else {
         o.dzmax = 0;
         o.laycost = 0;
@@ -576,7 +562,37 @@ __device__ __forceinline__ bool arc_fast(float ca, float cb, float dp, float av,
     off_i = min(max(off_i, (int)SHRT_MIN), (int)SHRT_MAX);
     o.off = (short)off_i;
     o.sigsq = (short)min(sg, (int)SHRT_MAX);
-    return true;
+    return ok;
+}
+
+/* the two columns of a pair: the arithmetic on both lanes at
+ * once (same roundings as the scalar forms), the decisions per lane.  Every
+ * candidate is computed and each margin test folds into one predicate (a
+ * NaN anywhere fails its test). */
+template <bool DEFO>
+__device__ __forceinline__ void arc_fast2(float2 ca, float2 cb, float2 dp, float2 av,
+                                          const CostConsts &k, const short *lay, int ntab,
+                                          ArcCost &o0, ArcCost &o1, bool &ok0, bool &ok1)
+{
+    const float2 half = f2(0.5f, 0.5f), one = f2(1.0f, 1.0f);
+    const float2 mg = f2(12582912.0f, 12582912.0f);
+    const float2 rho = __fmul2_rn(half, __fadd2_rn(ca, cb));
+    const float2 hav = __fmul2_rn(half, av);
+    const float2 sel = f2(rho.x >= k.thr_hi ? av.x : hav.x, rho.y >= k.thr_hi ? av.y : hav.y);
+    const float2 X = __fmul2_rn(sub2(dp, sel), f2(k.nsc_f, k.nsc_f));
+    const float2 XM = __fadd2_rn(X, mg);
+    const float2 f = sub2(X, sub2(XM, mg));
+    /* sigsq for rho > 0 (FP32 screen); rho = 0 uses the exact host value */
+    const float2 b = __fmul2_rn(half, __fadd2_rn(sub2(one, ca), sub2(one, cb)));
+    const float2 t = __fmul2_rn(f2(k.rhopow_f, k.rhopow_f), f2(lg2_ftz(b.x), lg2_ftz(b.y)));
+    const float2 v = __ffma2_rn(f2(k.a_f, k.a_f), f2(ex2_ftz(t.x), ex2_ftz(t.y)), f2(k.c_f, k.c_f));
+    const float2 vm = __fadd2_rn(sub2(v, half), mg);
+    const float2 fr = sub2(v, sub2(vm, mg));
+    const float2 m = __ffma2_rn(f2(k.screen_f, k.screen_f), v, f2(1e-6f, 1e-6f));
+    ok0 = arc_lane<DEFO>(ca.x, cb.x, rho.x, X.x, XM.x, f.x, b.x, v.x, vm.x, fr.x, m.x, k, lay,
+                         ntab, o0);
+    ok1 = arc_lane<DEFO>(ca.y, cb.y, rho.y, X.y, XM.y, f.y, b.y, v.y, vm.y, fr.y, m.y, k, lay,
+                         ntab, o1);
 }
 
 template <bool DEFO>
@@ -750,30 +766,28 @@ __global__ void __launch_bounds__(256, MINB) k_costs7(const float *__restrict__ 
         if (ar >= dr) break;
         const float2 avg = boxcar7(w + m);
         const float2 dps = S.dpp[(rs + m + 3) * kC7PP + j + 3];
+        const float2 ca2 = f2(sane(cv[0][m]), sane(cv[1][m]));
+        const float2 cb2 = FAM == 0 ? f2(sane(cv[0][m + 1]), sane(cv[1][m + 1]))
+                                    : f2(sane(cw[0][m]), sane(cw[1][m]));
+        ArcCost of[2];
+        bool okf[2] = {false, false};
+        if (fast) arc_fast2<DEFO>(ca2, cb2, dps, avg, k, S.lay, ntab, of[0], of[1], okf[0], okf[1]);
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int ac = c0 + j + h * kC7H;
             if (ac >= dc) continue;
             const float dpv = h ? dps.y : dps.x, avv = h ? avg.y : avg.x;
-            size_t a;
-            float ca, cb;
-            if (FAM == 0) {
-                a = (size_t)ar * ncol + ac;
-                ca = sane(cv[h][m]);
-                cb = sane(cv[h][m + 1]);
-            } else {
-                a = nra + (size_t)ar * (ncol - 1) + ac;
-                ca = sane(cv[h][m]);
-                cb = sane(cw[h][m]);
-            }
+            const float ca = h ? ca2.y : ca2.x, cb = h ? cb2.y : cb2.x;
+            const size_t a = FAM == 0 ? (size_t)ar * ncol + ac
+                                      : nra + (size_t)ar * (ncol - 1) + ac;
             const short wt = weights ? weights[a] : (short)1;
-            ArcCost o;
             if (wt == 0) {
+                ArcCost o;
                 o.off = kLargeShort / 2; o.sigsq = kLargeShort;
                 o.dzmax = kLargeShort; o.laycost = 0;
                 store_arc<DEFO>(costs_out, a, o);
-            } else if (fast && wt == 1 && arc_fast<DEFO>(ca, cb, dpv, avv, k, S.lay, ntab, o)) {
-                store_arc<DEFO>(costs_out, a, o);
+            } else if (wt == 1 && okf[h]) {
+                store_arc<DEFO>(costs_out, a, of[h]);
             } else {
                 const int slot = atomicAdd(&S.qn, 1);
                 if (slot < kC7Q) {
