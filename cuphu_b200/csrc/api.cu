@@ -60,11 +60,19 @@ static Workspace g_ws[64];
 
 static int ws_prepare(Workspace *W, size_t dbytes, size_t hbytes, cudaStream_t s)
 {
+    /* each member is set only once its creation succeeded, so a failed first
+     * call leaves nothing half-made for the next one */
+    if (!W->status) {
+        int *st = nullptr;
+        CUPHU_TRY_CUDA(cudaHostAlloc((void **)&st, sizeof(int), cudaHostAllocDefault));
+        *st = 0;
+        W->status = st;
+    }
     if (!W->done) {
-        CUPHU_TRY_CUDA(cudaEventCreateWithFlags(&W->done, cudaEventDisableTiming));
+        cudaEvent_t ev = nullptr;
+        CUPHU_TRY_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        W->done = ev;
         CUPHU_TRY_CUDA(cudaEventRecord(W->done, s));
-        CUPHU_TRY_CUDA(cudaHostAlloc((void **)&W->status, sizeof(int), cudaHostAllocDefault));
-        *W->status = 0;
     }
     if (dbytes > W->dev_size) {
         CUPHU_TRY_CUDA(cudaDeviceSynchronize());
@@ -117,6 +125,26 @@ static void ws_free(Workspace &W)
     W.dev = nullptr; W.host = nullptr; W.status = nullptr; W.done = nullptr;
     W.dev_size = W.host_size = 0;
 }
+
+/* the timing events of one call, destroyed on every return path */
+struct Timers {
+    cudaEvent_t e[4] = {nullptr, nullptr, nullptr, nullptr};
+    explicit Timers(int n)
+    {
+        for (int i = 0; i < n && i < 4; ++i)
+            if (cudaEventCreate(&e[i]) != cudaSuccess) {
+                e[i] = nullptr;
+                cudaGetLastError();
+            }
+    }
+    ~Timers()
+    {
+        for (cudaEvent_t x : e)
+            if (x) cudaEventDestroy(x);
+    }
+    Timers(const Timers &) = delete;
+    Timers &operator=(const Timers &) = delete;
+};
 
 /* a captured batch pipeline: its own workspace (the descriptors and device
  * pointers are baked into the graph) and the instantiated graph */
@@ -330,11 +358,9 @@ static int wls_job(const Plan &pl, SolverPlanes &P, const JobOpts &jo, cudaStrea
     sp.timeout_ns = (long long)std::max(1, o.timeout_ms) * 1000000LL;
     sp.wls = 1;
     sp.warm = jo.wls_u0 ? 1 : 0;
-    cudaEvent_t e1 = nullptr, e2 = nullptr;
-    if (stats) {
-        cudaEventCreate(&e1); cudaEventCreate(&e2);
-        cudaEventRecord(e1, s);
-    }
+    Timers tm(stats ? 2 : 0);
+    cudaEvent_t e1 = tm.e[0], e2 = tm.e[1];
+    if (stats) cudaEventRecord(e1, s);
     int rc = launch_solve(jo.fp64, d_tiles, d_item, pl.nitems, ntiles, P, pl.pitch, pl.total_rows,
                           d_st, d_part, d_ctl, sp, dev, s);
     if (rc) return rc;
@@ -355,7 +381,6 @@ static int wls_job(const Plan &pl, SolverPlanes &P, const JobOpts &jo, cudaStrea
         stats->solve_ms = ms;
         stats->total_ms = ms;
         stats->px_iters = (double)ctl.px_iters;
-        cudaEventDestroy(e1); cudaEventDestroy(e2);
         if (ctl.err) return fail(CUPHU_ERR_TIMEOUT, "solver grid barrier timed out");
     }
     return 0;
@@ -498,11 +523,9 @@ static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpt
     put(d_rowcnt + pl.total_rows, pl.row_tile.data(), pl.total_rows * sizeof(int));
     put(d_k, pl.consts.data(), nsc * sizeof(CostConsts));
 
-    cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
-    if (stats) {
-        cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2); cudaEventCreate(&e3);
-        cudaEventRecord(e0, s);
-    }
+    Timers tm(stats ? 4 : 0);
+    cudaEvent_t e0 = tm.e[0], e1 = tm.e[1], e2 = tm.e[2], e3 = tm.e[3];
+    if (stats) cudaEventRecord(e0, s);
     /* IRLS schedule, host powf exactly as cuphu_laplace.cu:517-518 */
     std::vector<float> deltas(o.n_irls + 1, 0.0f);
     for (int k = 0; k < o.n_irls; ++k)
@@ -601,7 +624,6 @@ static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpt
         stats->solve_ms = ms_solve;
         stats->total_ms = ms_total;
         stats->px_iters = (double)ctl.px_iters;
-        cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2); cudaEventDestroy(e3);
         if (ctl.err) return fail(CUPHU_ERR_TIMEOUT, "solver grid barrier timed out");
     }
     return cuda_fail(cudaGetLastError(), "unwrap pipeline");
@@ -904,11 +926,10 @@ int cuphu_autotune(const float *igram_c64, const float *corr, int nrow, int ncol
     float *d_ph = dev_alloc_async<float>(n, s), *d_unw = dev_alloc_async<float>(n, s);
     short *d_cost = dev_alloc_async<short>(narcs * es, s);
     if (!d_ig || !d_corr || !d_ph || !d_unw || !d_cost) rc = fail(CUPHU_ERR_ALLOC, "device allocation failed");
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    Timers tm(rc ? 0 : 2);
+    cudaEvent_t e0 = tm.e[0], e1 = tm.e[1];
     int best_cost = 0, best_blocks = 3;
     if (!rc) {
-        cudaEventCreate(&e0);
-        cudaEventCreate(&e1);
         cudaMemcpyAsync(d_ig, igram_c64, 8 * n, cudaMemcpyHostToDevice, s);
         cudaMemcpyAsync(d_corr, corr, 4 * n, cudaMemcpyHostToDevice, s);
         rc = launch_phase(reinterpret_cast<const float2 *>(d_ig), d_ph, (long long)n, s);
@@ -952,8 +973,6 @@ int cuphu_autotune(const float *igram_c64, const float *corr, int nrow, int ncol
     tune_force(1, -1);
     if (!rc && items > 0) tune_set(gpu_id, 1, items, best_blocks);
     cudaError_t e = cudaStreamSynchronize(s);
-    if (e0) cudaEventDestroy(e0);
-    if (e1) cudaEventDestroy(e1);
     cudaFreeAsync(d_ig, s); cudaFreeAsync(d_corr, s); cudaFreeAsync(d_ph, s);
     cudaFreeAsync(d_unw, s); cudaFreeAsync(d_cost, s);
     if (!rc && e != cudaSuccess) rc = cuda_fail(e, "cuphu_autotune");
