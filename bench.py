@@ -363,11 +363,16 @@ def run_reference(args, rank, world):
     v = float(np.mean([x[0] for x in vals]))
     ms = float(np.mean([x[1] for x in vals])) * 1e3
     cores = os.cpu_count()
+    nrow, ncol = g.shape
+    ntr, ntc = tiles_for(nrow, ncol)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mpix/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": args.workload, "sample": f"{n}x{n} crop, full pipeline"},
+            "config": {"workload": args.workload, "shape": [nrow, ncol], "tiles": [ntr, ntc],
+                       "overlap": 64, "n_irls": n_irls, "max_iter": 1000, "tol": 1e-3,
+                       "precision": "fp64", "parallelism": f"cpu{cores}",
+                       "sample": f"{n}x{n} crop, full pipeline"},
             "cpu_baseline": {"value": v, "unit": "Mpix/s", "cores": cores, "kind": "port",
                              "sample": f"{n}x{n} crop of the {args.workload} scene: cost build "
                                        f"+ FP64 Jacobi-PCG ({n_irls} IRLS passes) + conncomp, "
