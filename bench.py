@@ -479,8 +479,7 @@ def run_ours(args, rank, world, local_rank):
     # bytes = tile pixels x (36 B per PCG iteration x iterations of the
     # active tiles + 38 B per IRLS pass for assemble and reweight)
     peak, peak_kind = hbm_peak()
-    tile_px = 0
-    from cuphu_b200._unwrap import _auto_ntiles_by_target_size  # noqa: F401
+    # tile extents of the reference's tile geometry (cuphu_solver.cpp:1753-1791)
     tr_f = [(int(t * (nrow - 64) / ntr), (nrow if t == ntr - 1 else int((t + 1) * (nrow - 64) / ntr) + 64)) for t in range(ntr)]
     tc_f = [(int(t * (ncol - 64) / ntc), (ncol if t == ntc - 1 else int((t + 1) * (ncol - 64) / ntc) + 64)) for t in range(ntc)]
     tile_px = sum((b - a) for a, b in tr_f) * sum((b - a) for a, b in tc_f)
