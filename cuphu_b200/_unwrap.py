@@ -9,6 +9,7 @@ reference behaviour.
 """
 from __future__ import annotations
 
+import ctypes as C
 import os
 
 import numpy as np
@@ -177,7 +178,6 @@ def unwrap(igram, corr, nlooks, cost="smooth", init="mcf", *, mask=None, mask_pa
     unw_out = np.empty((nrow, ncol), dtype=np.float32)
     cc_out = np.empty((nrow, ncol), dtype=np.uint32)
     st = CuPhuSolveStats()
-    import ctypes as C
     check(lib().cuphu_unwrap_ex(ptr(igram_c64.view(np.float32)), ptr(corr_f32),
                                 ptr(solve_mask_u8), ptr(mask_u8), nrow, ncol, _COST[cost],
                                 C.byref(params), C.byref(tile), C.byref(opts), int(gpu_id),
