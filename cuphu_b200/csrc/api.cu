@@ -41,7 +41,18 @@ int cuda_fail(cudaError_t e, const char *what)
 {
     if (e == cudaSuccess) return 0;
     g_err = std::string(what) + ": " + cudaGetErrorString(e);
+    /* the error is reported now: clear the thread's last-error state so a
+     * later call's cudaGetLastError check does not report it again */
+    cudaGetLastError();
     return CUPHU_ERR_CUDA;
+}
+
+/* an asynchronous copy whose immediate error (a bad pointer or size)
+ * becomes the call's status instead of passing unnoticed */
+static int copy_async(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind,
+                      cudaStream_t s, const char *what)
+{
+    return cuda_fail(cudaMemcpyAsync(dst, src, bytes, kind, s), what);
 }
 
 /* ── per-device workspace ──────────────────────────────────────────────── */
@@ -930,9 +941,9 @@ int cuphu_autotune(const float *igram_c64, const float *corr, int nrow, int ncol
     cudaEvent_t e0 = tm.e[0], e1 = tm.e[1];
     int best_cost = 0, best_blocks = 3;
     if (!rc) {
-        cudaMemcpyAsync(d_ig, igram_c64, 8 * n, cudaMemcpyHostToDevice, s);
-        cudaMemcpyAsync(d_corr, corr, 4 * n, cudaMemcpyHostToDevice, s);
-        rc = launch_phase(reinterpret_cast<const float2 *>(d_ig), d_ph, (long long)n, s);
+        rc = copy_async(d_ig, igram_c64, 8 * n, cudaMemcpyHostToDevice, s, "H2D igram");
+        if (!rc) rc = copy_async(d_corr, corr, 4 * n, cudaMemcpyHostToDevice, s, "H2D corr");
+        if (!rc) rc = launch_phase(reinterpret_cast<const float2 *>(d_ig), d_ph, (long long)n, s);
     }
     /* cost kernel: 3 or 4 blocks per SM (identical results) */
     float best_ms = 1e30f;
@@ -1001,17 +1012,18 @@ int cuphu_unwrap_ex(const float *igram_c64, const float *corr, const unsigned ch
     if (!d_ig || !d_corr || !d_unw || !d_cc || (mask && !d_mask) || (orig_mask && !d_om))
         rc = fail(CUPHU_ERR_ALLOC, "device allocation failed");
     if (!rc) {
-        cudaMemcpyAsync(d_ig, igram_c64, 8 * n, cudaMemcpyHostToDevice, s);
-        cudaMemcpyAsync(d_corr, corr, 4 * n, cudaMemcpyHostToDevice, s);
-        if (mask) cudaMemcpyAsync(d_mask, mask, n, cudaMemcpyHostToDevice, s);
-        if (orig_mask) cudaMemcpyAsync(d_om, orig_mask, n, cudaMemcpyHostToDevice, s);
+        rc = copy_async(d_ig, igram_c64, 8 * n, cudaMemcpyHostToDevice, s, "H2D igram");
+        if (!rc) rc = copy_async(d_corr, corr, 4 * n, cudaMemcpyHostToDevice, s, "H2D corr");
+        if (!rc && mask) rc = copy_async(d_mask, mask, n, cudaMemcpyHostToDevice, s, "H2D mask");
+        if (!rc && orig_mask)
+            rc = copy_async(d_om, orig_mask, n, cudaMemcpyHostToDevice, s, "H2D orig_mask");
+    }
+    if (!rc) {
         rc = cuphu_unwrap_device(d_ig, nullptr, d_corr, d_mask, d_om, nrow, ncol, cost_mode, params,
                                  tile, opts, d_unw, d_cc, nullptr, stats, s);
     }
-    if (!rc) {
-        cudaMemcpyAsync(unw_out, d_unw, 4 * n, cudaMemcpyDeviceToHost, s);
-        cudaMemcpyAsync(conncomp_out, d_cc, 4 * n, cudaMemcpyDeviceToHost, s);
-    }
+    if (!rc) rc = copy_async(unw_out, d_unw, 4 * n, cudaMemcpyDeviceToHost, s, "D2H unw");
+    if (!rc) rc = copy_async(conncomp_out, d_cc, 4 * n, cudaMemcpyDeviceToHost, s, "D2H conncomp");
     cudaError_t e = cudaStreamSynchronize(s);
     cudaFreeAsync(d_ig, s); cudaFreeAsync(d_corr, s); cudaFreeAsync(d_unw, s); cudaFreeAsync(d_cc, s);
     if (d_mask) cudaFreeAsync(d_mask, s);
@@ -1066,12 +1078,13 @@ int cuphu_unwrap(const float *igram_r, const float *igram_i, const float *corr, 
         (orig_mask && !d_om))
         rc = fail(CUPHU_ERR_ALLOC, "device allocation failed");
     if (!rc) {
-        cudaMemcpyAsync(d_re, igram_r, 4 * n, cudaMemcpyHostToDevice, s);
-        cudaMemcpyAsync(d_im, igram_i, 4 * n, cudaMemcpyHostToDevice, s);
-        cudaMemcpyAsync(d_corr, corr, 4 * n, cudaMemcpyHostToDevice, s);
-        if (mask) cudaMemcpyAsync(d_mask, mask, n, cudaMemcpyHostToDevice, s);
-        if (orig_mask) cudaMemcpyAsync(d_om, orig_mask, n, cudaMemcpyHostToDevice, s);
-        rc = launch_phase_split(d_re, d_im, d_ph, (long long)n, s);
+        rc = copy_async(d_re, igram_r, 4 * n, cudaMemcpyHostToDevice, s, "H2D igram_r");
+        if (!rc) rc = copy_async(d_im, igram_i, 4 * n, cudaMemcpyHostToDevice, s, "H2D igram_i");
+        if (!rc) rc = copy_async(d_corr, corr, 4 * n, cudaMemcpyHostToDevice, s, "H2D corr");
+        if (!rc && mask) rc = copy_async(d_mask, mask, n, cudaMemcpyHostToDevice, s, "H2D mask");
+        if (!rc && orig_mask)
+            rc = copy_async(d_om, orig_mask, n, cudaMemcpyHostToDevice, s, "H2D orig_mask");
+        if (!rc) rc = launch_phase_split(d_re, d_im, d_ph, (long long)n, s);
     }
     if (!rc) {
         CuPhuSolveOptions so;
@@ -1080,10 +1093,9 @@ int cuphu_unwrap(const float *igram_r, const float *igram_i, const float *corr, 
         rc = cuphu_unwrap_device(nullptr, d_ph, d_corr, d_mask, d_om, nrow, ncol, cost_mode, &p,
                                  tile, &so, d_unw, d_cc, nullptr, nullptr, s);
     }
-    if (!rc) {
-        cudaMemcpyAsync(result->unw, d_unw, 4 * n, cudaMemcpyDeviceToHost, s);
-        cudaMemcpyAsync(result->conncomp, d_cc, 4 * n, cudaMemcpyDeviceToHost, s);
-    }
+    if (!rc) rc = copy_async(result->unw, d_unw, 4 * n, cudaMemcpyDeviceToHost, s, "D2H unw");
+    if (!rc)
+        rc = copy_async(result->conncomp, d_cc, 4 * n, cudaMemcpyDeviceToHost, s, "D2H conncomp");
     cudaError_t e = cudaStreamSynchronize(s);
     cudaFreeAsync(d_re, s); cudaFreeAsync(d_im, s); cudaFreeAsync(d_corr, s);
     cudaFreeAsync(d_unw, s); cudaFreeAsync(d_ph, s); cudaFreeAsync(d_cc, s);
@@ -1198,16 +1210,17 @@ int cuphu_build_costs_gpu(const float *igram_r, const float *igram_i, const floa
     if (!d_re || !d_im || !d_corr || !d_ph || !d_c || (weights && !d_w) || !h)
         rc = fail(CUPHU_ERR_ALLOC, "allocation failed");
     if (!rc) {
-        cudaMemcpyAsync(d_re, igram_r, 4 * n, cudaMemcpyHostToDevice, s);
-        cudaMemcpyAsync(d_im, igram_i, 4 * n, cudaMemcpyHostToDevice, s);
-        cudaMemcpyAsync(d_corr, corr, 4 * n, cudaMemcpyHostToDevice, s);
-        if (weights) cudaMemcpyAsync(d_w, weights, 2 * narcs, cudaMemcpyHostToDevice, s);
-        rc = launch_phase_split(d_re, d_im, d_ph, (long long)n, s);
+        rc = copy_async(d_re, igram_r, 4 * n, cudaMemcpyHostToDevice, s, "H2D igram_r");
+        if (!rc) rc = copy_async(d_im, igram_i, 4 * n, cudaMemcpyHostToDevice, s, "H2D igram_i");
+        if (!rc) rc = copy_async(d_corr, corr, 4 * n, cudaMemcpyHostToDevice, s, "H2D corr");
+        if (!rc && weights)
+            rc = copy_async(d_w, weights, 2 * narcs, cudaMemcpyHostToDevice, s, "H2D weights");
+        if (!rc) rc = launch_phase_split(d_re, d_im, d_ph, (long long)n, s);
     }
     if (!rc)
         rc = launch_costs(d_ph, d_corr, d_w, nrow, ncol, cost_mode == CUPHU_COST_SMOOTH ? 0 : 1,
                           *params, d_c, nullptr, s);
-    if (!rc) cudaMemcpyAsync(h, d_c, narcs * es, cudaMemcpyDeviceToHost, s);
+    if (!rc) rc = copy_async(h, d_c, narcs * es, cudaMemcpyDeviceToHost, s, "D2H costs");
     cudaError_t e = cudaStreamSynchronize(s);
     cudaFreeAsync(d_re, s); cudaFreeAsync(d_im, s); cudaFreeAsync(d_corr, s);
     cudaFreeAsync(d_ph, s); cudaFreeAsync(d_c, s);
@@ -1420,13 +1433,15 @@ int cuphu_conncomp_ex(const float *unw, const float *corr, const unsigned char *
     int rc = 0;
     if (!du || !dc || !dl || (mask && !dm)) rc = fail(CUPHU_ERR_ALLOC, "device allocation failed");
     if (!rc) {
-        cudaMemcpyAsync(du, unw, 4 * n, cudaMemcpyHostToDevice, s);
-        cudaMemcpyAsync(dc, corr, 4 * n, cudaMemcpyHostToDevice, s);
-        if (mask) cudaMemcpyAsync(dm, mask, n, cudaMemcpyHostToDevice, s);
+        rc = copy_async(du, unw, 4 * n, cudaMemcpyHostToDevice, s, "H2D unw");
+        if (!rc) rc = copy_async(dc, corr, 4 * n, cudaMemcpyHostToDevice, s, "H2D corr");
+        if (!rc && mask) rc = copy_async(dm, mask, n, cudaMemcpyHostToDevice, s, "H2D mask");
+    }
+    if (!rc) {
         rc = conncomp_scene(du, dc, dm, nrow, ncol, nullptr, nullptr, corr_thresh, 0, minfrac,
                             maxncomps, dl, s);
     }
-    if (!rc) cudaMemcpyAsync(labels_out, dl, 4 * n, cudaMemcpyDeviceToHost, s);
+    if (!rc) rc = copy_async(labels_out, dl, 4 * n, cudaMemcpyDeviceToHost, s, "D2H labels");
     cudaError_t e = cudaStreamSynchronize(s);
     cudaFreeAsync(du, s); cudaFreeAsync(dc, s); cudaFreeAsync(dl, s);
     if (dm) cudaFreeAsync(dm, s);
