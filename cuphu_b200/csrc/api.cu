@@ -692,10 +692,22 @@ static int device_status(int dev)
     return 0;
 }
 
+/* the library's own stream on device dev, created once (threads that call
+ * the host-buffer entry points at the same time share it); the legacy
+ * default stream if it cannot be created */
+static std::mutex g_stream_mu;
 static cudaStream_t lib_stream(int dev)
 {
+    if (dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lk(g_stream_mu);
     Workspace &W = g_ws[dev];
-    if (!W.stream) cudaStreamCreateWithFlags(&W.stream, cudaStreamNonBlocking);
+    if (!W.stream) {
+        cudaStream_t st = nullptr;
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess)
+            W.stream = st;
+        else
+            cudaGetLastError();
+    }
     return W.stream;
 }
 
