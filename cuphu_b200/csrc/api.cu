@@ -492,6 +492,7 @@ static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpt
         W = &jo.graph->ws;
         rc = ws_prepare(W, dbytes, hbytes, s);
     } else {
+        if (dev < 0 || dev >= 64) return fail(CUPHU_ERR_UNSUPPORTED, "device ordinal above 63");
         lock = std::unique_lock<std::mutex>(g_ws[dev].mu);
         rc = ws_acquire(dev, dbytes, hbytes, s, W);
     }
@@ -684,6 +685,7 @@ static int check_tile_flags(const CuPhuTileParams *t)
 /* status of the last pipeline on a device, after its work completed */
 static int device_status(int dev)
 {
+    if (dev < 0 || dev >= 64) return 0;
     Workspace &W = g_ws[dev];
     if (!W.done) return 0;
     CUPHU_TRY_CUDA(cudaEventSynchronize(W.done));
@@ -1519,14 +1521,20 @@ int cuphu_release_workspace(int gpu_id)
     if (gpu_id < 0 || gpu_id >= 64) return fail(CUPHU_ERR_INVALID, "device index out of range");
     Workspace &W = g_ws[gpu_id];
     std::lock_guard<std::mutex> lock(W.mu);
-    CUPHU_TRY_CUDA(cudaSetDevice(gpu_id));
-    CUPHU_TRY_CUDA(cudaDeviceSynchronize());
-    if (W.dev) cudaFree(W.dev);
-    if (W.host) cudaFreeHost(W.host);
-    W.dev = nullptr;
-    W.host = nullptr;
-    W.dev_size = W.host_size = 0;
-    return 0;
+    /* the caller's current device is restored on return */
+    int prev = -1;
+    CUPHU_TRY_CUDA(cudaGetDevice(&prev));
+    int rc = cuda_fail(cudaSetDevice(gpu_id), "cudaSetDevice");
+    if (!rc) rc = cuda_fail(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+    if (!rc) {
+        if (W.dev) cudaFree(W.dev);
+        if (W.host) cudaFreeHost(W.host);
+        W.dev = nullptr;
+        W.host = nullptr;
+        W.dev_size = W.host_size = 0;
+    }
+    cudaSetDevice(prev);
+    return rc;
 }
 
 }  /* extern "C" */
