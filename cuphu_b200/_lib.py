@@ -178,28 +178,33 @@ def check(code: int) -> int:
     return code
 
 
+def _override(s, kw):
+    """Set struct fields by name; an unknown name is an error, not a new
+    Python attribute the library never sees."""
+    names = {f[0] for f in type(s)._fields_}
+    for k, v in kw.items():
+        if k not in names:
+            raise TypeError(f"{type(s).__name__} has no field {k!r}")
+        setattr(s, k, v)
+    return s
+
+
 def default_params(**kw) -> CuPhuParams:
     p = CuPhuParams()
     lib().cuphu_default_params(C.byref(p))
-    for k, v in kw.items():
-        setattr(p, k, v)
-    return p
+    return _override(p, kw)
 
 
 def default_tile_params(**kw) -> CuPhuTileParams:
     t = CuPhuTileParams()
     lib().cuphu_default_tile_params(C.byref(t))
-    for k, v in kw.items():
-        setattr(t, k, v)
-    return t
+    return _override(t, kw)
 
 
 def default_solve_options(**kw) -> CuPhuSolveOptions:
     o = CuPhuSolveOptions()
     lib().cuphu_default_solve_options(C.byref(o))
-    for k, v in kw.items():
-        setattr(o, k, v)
-    return o
+    return _override(o, kw)
 
 
 def ptr(a):

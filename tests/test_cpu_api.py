@@ -48,6 +48,12 @@ def test_defaults_and_no_gpu_queries():
     assert o.n_irls == int(os.environ.get("CUPHU_N_IRLS", 16))
     t = _lib.default_tile_params()
     assert (t.ntilerow, t.ntilecol, t.tilecostthresh, t.minregionsize) == (1, 1, 500, 100)
+    # a misspelt override is an error, not a silent Python-side attribute
+    assert _lib.default_params(nlooks=5.0).nlooks == 5.0
+    for make, bad in ((_lib.default_params, "nlook"), (_lib.default_tile_params, "ntilerows"),
+                      (_lib.default_solve_options, "nirls")):
+        with pytest.raises(TypeError):
+            make(**{bad: 1})
 
 
 REF_H = os.path.join(os.environ.get("CUPHU_REFERENCE_ROOT", "/root/reference"),
