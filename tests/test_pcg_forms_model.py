@@ -1,0 +1,132 @@
+"""A numpy model of the mixed-precision Jacobi-PCG arithmetic (FP32 vectors
+and stencil, FP64 dot products, true-residual replacement every 50
+iterations, 16 IRLS passes) in two forms, against the FP64 oracle on CPU.
+
+* two-pass: the form the solver kernel runs (stencil pass, then an update
+  pass that recomputes rz = (r, z) from the updated z);
+* single-synchronisation: one pass per iteration.  The stencil pass applies
+  the previous update z' = z - a q/diag and fold p' = z' + b p itself and
+  reduces (p,q), diag z'^2, (z',q) and (q,q/diag) in one reduction: a and the
+  stop test use the true rz = sum diag z'^2, and b uses the one-step
+  recurrence rz_next = rz - 2a (z',q) + a^2 (q,q/diag).
+
+The model decides whether the single-synchronisation form may replace the
+two-pass form: it must keep the FP64 oracle's iteration counts and cycle
+map as the two-pass form does.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from cuphu_b200 import synthetic as S
+
+f32, f64 = np.float32, np.float64
+TWOPI_F = f32(6.28318548202514648)
+INV_TWOPI_F = f32(0.15915494309189534561)
+EPS = f32(1e-12)
+REPLACE_EVERY = 50
+
+
+def _wrap(x):
+    k = np.rint((x * INV_TWOPI_F).astype(f32)).astype(f64)
+    return (x.astype(f64) - f64(TWOPI_F) * k).astype(f32)
+
+
+def _matvec(wd, wr, x, dt):
+    x = x.astype(dt)
+    y = (dt(EPS) * x).astype(dt)
+    d = (wd.astype(dt) * (x[:-1] - x[1:])).astype(dt)
+    y[:-1] += d
+    y[1:] -= d
+    d = (wr.astype(dt) * (x[:, :-1] - x[:, 1:])).astype(dt)
+    y[:, :-1] += d
+    y[:, 1:] -= d
+    return y
+
+
+def _dot(a, b):
+    return float(np.dot(a.astype(f64).ravel(), b.astype(f64).ravel()))
+
+
+def _pcg(wd, wr, b, diag, x, tol, max_iter, single):
+    d32 = diag.astype(f32)
+    z = ((b - _matvec(wd, wr, x, f64)) / diag).astype(f32)
+    rz = _dot(z * d32, z)
+    if rz <= 0:
+        return x, 0
+    thr = tol * tol * rz
+    p = z.copy()
+    dx = np.zeros(x.shape, f32)
+    it = 0
+    for it in range(1, max_iter + 1):
+        q = _matvec(wd, wr, p, f32)
+        pq = _dot(p, q)
+        if pq <= 0:
+            it -= 1
+            break
+        a = rz / pq
+        if single:
+            rz_rec = rz - 2 * a * _dot(z, q) + a * a * _dot(q, (q / d32).astype(f32))
+        dx = (dx + f32(a) * p).astype(f32)
+        z = (z - f32(a) * q / d32).astype(f32)
+        replaced = it % REPLACE_EVERY == 0
+        if replaced:
+            x = x + dx.astype(f64)
+            dx[:] = 0
+            z = ((b - _matvec(wd, wr, x, f64)) / diag).astype(f32)
+        rzn = _dot(z * d32, z)
+        if rzn < thr:
+            break
+        beta = (rz_rec if single and not replaced else rzn) / rz
+        rz = rzn
+        p = (z + f32(beta) * p).astype(f32)
+    return x + dx.astype(f64), it
+
+
+def _irls(costs, ph, n_irls, single, tol=1e-3, max_iter=1000):
+    nr, nc = ph.shape
+    nra = (nr - 1) * nc
+    s = costs[:, 1].astype(np.int32)
+    w0 = np.where((s > 0) & (s < 32000), f32(1) / s.astype(f32), f32(0)).astype(f32)
+    w0d, w0r = w0[:nra].reshape(nr - 1, nc), w0[nra:].reshape(nr, nc - 1)
+    wd, wr = w0d.copy(), w0r.copy()
+    gd = _wrap(ph[1:] - ph[:-1]).astype(f64)
+    gr = _wrap(ph[:, 1:] - ph[:, :-1]).astype(f64)
+    x = np.zeros(ph.shape, f64)
+    its = []
+    for outer in range(n_irls + 1):
+        wd64, wr64 = wd.astype(f64), wr.astype(f64)
+        b = np.zeros(ph.shape, f64)
+        b[:-1] -= wd64 * gd
+        b[1:] += wd64 * gd
+        b[:, :-1] -= wr64 * gr
+        b[:, 1:] += wr64 * gr
+        diag = np.full(ph.shape, f64(EPS))
+        diag[:-1] += wd64
+        diag[1:] += wd64
+        diag[:, :-1] += wr64
+        diag[:, 1:] += wr64
+        x, it = _pcg(wd, wr, b, diag, x, tol, max_iter, single)
+        its.append(it)
+        if outer < n_irls:
+            dd = f64(max(f32(0.01), f32(0.5) * f32(0.5 ** outer))) ** 2
+            ed = (x[1:] - x[:-1]) - gd
+            er = (x[:, 1:] - x[:, :-1]) - gr
+            wd = np.where(w0d > 0, w0d / np.sqrt(ed * ed + dd), 0).astype(f32)
+            wr = np.where(w0r > 0, w0r / np.sqrt(er * er + dd), 0).astype(f32)
+    off = f64(ph[0, 0]) - x[0, 0]
+    k = np.rint(((x + off) - ph.astype(f64)) / (2 * np.pi)).astype(np.int32)
+    return k, its
+
+
+@pytest.mark.parametrize("n", [128, 192])
+@pytest.mark.parametrize("single", [False, True])
+def test_pcg_forms_keep_the_fp64_iterations_and_cycle_map(n, single):
+    ig, g, _, ex = S.config_scene("c0_512_defo", seed=0)
+    ph = O.phase_from_igram(np.ascontiguousarray(ig[:n, :n]))
+    g = np.ascontiguousarray(g[:n, :n])
+    costs = O.build_costs(ph, g, float(ex["nlooks"]), mode=0)
+    _, k64, _, it64 = O.laplace_f64(costs, ph, O.lap_opts(n_irls=16))
+    k, its = _irls(costs, ph, 16, single)
+    assert its == it64.tolist()
+    assert np.array_equal(k, k64)
