@@ -629,9 +629,6 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
-    if args.workload == "c3_batch48":
-        run_batch(args, rank, world, local_rank)
-        return
     if world > 1:
         import datetime
 
@@ -640,7 +637,10 @@ def main():
         torch.cuda.set_device(local_rank)
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     try:
-        run_ours(args, rank, world, local_rank)
+        if args.workload == "c3_batch48":
+            run_batch(args, rank, world, local_rank)
+        else:
+            run_ours(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as tdist
