@@ -1,56 +1,80 @@
-"""Input validation (mirrors the reference's cuphu/_check.py, same messages)."""
+"""Input validation of ``unwrap()``.
+
+The exception types and messages are part of the drop-in: callers and the
+reference's test suite match on them (test_unwrap.py:44-80: "cost must be",
+"init must be", "2-D", "shape", "complex", "floating").  The rules are kept
+in two tables -- one predicate per dtype family, one set of choices per
+string option -- and every public checker is a thin call into them.
+"""
 import numpy as np
+
+_MASK_DTYPES = (np.dtype("bool"), np.dtype("uint8"), np.dtype("int8"))
+
+# dtype family -> (accepts(dtype), what the message says the array must be)
+_DTYPE_RULES = {
+    "complex": (lambda dt: np.issubdtype(dt, np.complexfloating), "complex"),
+    "float": (lambda dt: np.issubdtype(dt, np.floating), "floating-point"),
+    "integer": (lambda dt: np.issubdtype(dt, np.integer), "integer"),
+    "mask": (lambda dt: dt in _MASK_DTYPES, "bool or 8-bit integer"),
+}
+
+# string option -> accepted values
+_CHOICES = {
+    "cost": frozenset(("smooth", "defo", "topo")),
+    "init": frozenset(("mst", "mcf", "laplace")),
+}
+
+
+def _require_dtype(family, arrays):
+    accepts, what = _DTYPE_RULES[family]
+    for name, arr in arrays.items():
+        dt = np.asarray(arr).dtype
+        if not accepts(dt):
+            raise TypeError(f"{name} must be {what}, got dtype={dt}")
+
+
+def _require_choice(option, value):
+    valid = set(_CHOICES[option])
+    if value not in valid:
+        raise ValueError(f"{option} must be one of {valid}, got {value!r}")
 
 
 def check_2d_shape(arr, name):
-    arr = np.asarray(arr)
-    if arr.ndim != 2:
-        raise ValueError(f"{name} must be 2-D, got ndim={arr.ndim}")
-    return int(arr.shape[0]), int(arr.shape[1])
+    """(nrow, ncol) of ``arr``; ValueError unless it is 2-D."""
+    ndim = np.ndim(arr)
+    if ndim != 2:
+        raise ValueError(f"{name} must be 2-D, got ndim={ndim}")
+    shape = np.shape(arr)
+    return int(shape[0]), int(shape[1])
 
 
-def check_shape_match(ref_shape, **kwargs):
-    for name, arr in kwargs.items():
-        arr = np.asarray(arr)
-        if arr.shape != ref_shape:
-            raise ValueError(f"{name} shape {arr.shape} does not match expected {ref_shape}")
+def check_shape_match(ref_shape, **arrays):
+    """ValueError naming the first array whose shape is not ``ref_shape``."""
+    for name, arr in arrays.items():
+        shape = np.shape(arr)
+        if shape != ref_shape:
+            raise ValueError(f"{name} shape {shape} does not match expected {ref_shape}")
 
 
-def check_complex_dtype(**kwargs):
-    for name, arr in kwargs.items():
-        arr = np.asarray(arr)
-        if not np.issubdtype(arr.dtype, np.complexfloating):
-            raise TypeError(f"{name} must be complex, got dtype={arr.dtype}")
+def check_complex_dtype(**arrays):
+    _require_dtype("complex", arrays)
 
 
-def check_float_dtype(**kwargs):
-    for name, arr in kwargs.items():
-        arr = np.asarray(arr)
-        if not np.issubdtype(arr.dtype, np.floating):
-            raise TypeError(f"{name} must be floating-point, got dtype={arr.dtype}")
+def check_float_dtype(**arrays):
+    _require_dtype("float", arrays)
 
 
-def check_integer_dtype(**kwargs):
-    for name, arr in kwargs.items():
-        arr = np.asarray(arr)
-        if not np.issubdtype(arr.dtype, np.integer):
-            raise TypeError(f"{name} must be integer, got dtype={arr.dtype}")
+def check_integer_dtype(**arrays):
+    _require_dtype("integer", arrays)
 
 
-def check_bool_or_byte_dtype(**kwargs):
-    for name, arr in kwargs.items():
-        arr = np.asarray(arr)
-        if arr.dtype not in (np.dtype("bool"), np.dtype("uint8"), np.dtype("int8")):
-            raise TypeError(f"{name} must be bool or 8-bit integer, got dtype={arr.dtype}")
+def check_bool_or_byte_dtype(**arrays):
+    _require_dtype("mask", arrays)
 
 
 def check_cost_mode(cost):
-    valid = {"smooth", "defo", "topo"}
-    if cost not in valid:
-        raise ValueError(f"cost must be one of {valid}, got {cost!r}")
+    _require_choice("cost", cost)
 
 
 def check_init_method(init):
-    valid = {"mst", "mcf", "laplace"}
-    if init not in valid:
-        raise ValueError(f"init must be one of {valid}, got {init!r}")
+    _require_choice("init", init)

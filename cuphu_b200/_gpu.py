@@ -16,10 +16,11 @@ def gpu_name(device_id: int = 0) -> str:
 
 
 def gpu_info(device_id: int = 0) -> dict:
+    """Device properties under the reference's keys (cuphu_py.cu:445-456):
+    name, total_memory (bytes), sm_count and compute_cap ("major.minor")."""
     mem = C.c_longlong()
     sms, ma, mi = C.c_int(), C.c_int(), C.c_int()
     check(lib().cuphu_gpu_info(int(device_id), C.byref(mem), C.byref(sms), C.byref(ma),
                                C.byref(mi)))
     return {"name": gpu_name(device_id), "total_memory": int(mem.value),
-            "multiprocessor_count": int(sms.value),
-            "compute_capability": (int(ma.value), int(mi.value))}
+            "sm_count": int(sms.value), "compute_cap": f"{int(ma.value)}.{int(mi.value)}"}

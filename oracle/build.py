@@ -20,6 +20,8 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+# the reference checkout read by this recipe (and by the CPU tests that
+# compare against the reference's own sources); CUPHU_REFERENCE_ROOT moves it
 REF_ROOT = os.environ.get("CUPHU_REFERENCE_ROOT", "/root/reference")
 REF_SRC = os.path.join(REF_ROOT, "src", "cxx", "cuphu")
 REF_KERNELS = ["cuphu_util.cu", "cuphu_cost.cu", "cuphu_laplace.cu", "cuphu_phase.cu",

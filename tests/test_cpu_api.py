@@ -11,6 +11,8 @@ import subprocess
 import numpy as np
 import pytest
 
+from oracle.build import REF_ROOT
+
 import cuphu_b200 as cuphu
 from cuphu_b200 import _lib
 from cuphu_b200._check import check_cost_mode, check_init_method
@@ -56,8 +58,7 @@ def test_defaults_and_no_gpu_queries():
             make(**{bad: 1})
 
 
-REF_H = os.path.join(os.environ.get("CUPHU_REFERENCE_ROOT", "/root/reference"),
-                     "src/cxx/cuphu/cuphu.h")
+REF_H = os.path.join(REF_ROOT, "src/cxx/cuphu/cuphu.h")
 
 
 @pytest.mark.skipif(not os.path.exists(REF_H), reason="reference header not present")

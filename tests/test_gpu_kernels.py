@@ -78,10 +78,10 @@ def test_costs_match_reference_kernels(torch_cuda, shape, mode):
     assert np.array_equal(got, ref), f"{np.sum(np.any(got != ref, axis=1))} arcs differ"
 
 
-def test_costs_persistent_blocks_take_several_tiles(torch_cuda):
+def test_costs_more_arc_tiles_than_resident_blocks(torch_cuda):
     """1500 x 1400 has more 64 x 64 arc tiles per family than there are
-    resident blocks, so every block of the persistent cost kernel walks
-    several tiles through both of its prefetch buffers."""
+    resident blocks, so the cost kernel's grid runs in several waves and the
+    launch-wide queue of undecided arcs collects entries from all of them."""
     _, ph, g = _scene(1500, 1400, seed=91, nlooks=9.0)
     for mode in (0, 1):
         got = gpu_costs(torch_cuda, ph, g, 9.0, mode)
