@@ -218,6 +218,43 @@ def unwrap_tiled(phase, corr, nlooks, mode=0, mask=None, conf_mask=None, ntiles=
     return unw, cc, tk
 
 
+def fix_cycle_spikes(unw, mask=None):
+    """The reference's isolated row/column whole-cycle spike correction on a
+    copy of ``unw`` (cuphu_solver.cpp:1385-1441)."""
+    out = np.array(unw, dtype=np.float32, order="C", copy=True)
+    m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+    lib().orc_fix_cycle_spikes(_p(out), _p(m), out.shape[0], out.shape[1])
+    return out
+
+
+def neighbor_feedback(unw, ntiles, overlap, feather=200, mask=None):
+    """The reference's Laplace tile-boundary refinement on a copy of ``unw``
+    (cuphu_solver.cpp:1469-1656)."""
+    out = np.array(unw, dtype=np.float32, order="C", copy=True)
+    m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+    lib().orc_neighbor_feedback(_p(out), _p(m), out.shape[0], out.shape[1], int(ntiles[0]),
+                                int(ntiles[1]), int(overlap[0]), int(overlap[1]), int(feather))
+    return out
+
+
+RAMPS = (None, "linear", "quadratic", "linear_range", "linear_azimuth", "quadratic_range",
+         "quadratic_azimuth")
+
+
+def bridge(unw, mask=None, radius=500, min_num_pixel=14, erosion_size=2,
+           max_boundary_samples=4096, ramp_type=None, ramp_max_num_sample=1000000):
+    """The reference's phase bridging (cuphu_solver.cpp:996-1352) on a copy of
+    ``unw``.  Returns (unw, conncomp); conncomp is zero when there was
+    nothing to bridge."""
+    out = np.array(unw, dtype=np.float32, order="C", copy=True)
+    cc = np.zeros(out.shape, np.uint32)
+    m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+    lib().orc_bridge(_p(out), _p(cc), out.shape[0], out.shape[1], _p(m), int(radius),
+                     int(min_num_pixel), int(erosion_size), int(max_boundary_samples),
+                     RAMPS.index(ramp_type), int(ramp_max_num_sample))
+    return out, cc
+
+
 def dot_canonical(a, b):
     a = np.ascontiguousarray(a, np.float64)
     b = np.ascontiguousarray(b, np.float64)

@@ -1,7 +1,9 @@
 """Build recipe for the test oracle (TEST INFRASTRUCTURE ONLY).
 
 Produces
-  oracle/_build/libcuphu_oracle.so  -- the C restatement (gcc, OpenMP,
+  oracle/_build/libcuphu_oracle.so  -- the C restatement (cuphu_oracle.c,
+                                       cuphu_oracle_post.c, cuphu_oracle_bridge.c;
+                                       gcc, OpenMP,
                                        -ffp-contract=off so only the explicit
                                        fma() calls fuse)
   oracle/_ref/libcuphu_ref.so       -- the reference cuPHU hot-path kernels,
@@ -46,11 +48,12 @@ def build_oracle(force: bool = False) -> str:
     out_dir = os.path.join(HERE, "_build")
     os.makedirs(out_dir, exist_ok=True)
     out = os.path.join(out_dir, "libcuphu_oracle.so")
-    src = os.path.join(HERE, "cuphu_oracle.c")
+    srcs = [os.path.join(HERE, n) for n in ("cuphu_oracle.c", "cuphu_oracle_post.c",
+                                             "cuphu_oracle_bridge.c")]
     hdr = os.path.join(HERE, "cuphu_oracle.h")
-    if force or _stale(out, [src, hdr, __file__]):
+    if force or _stale(out, srcs + [hdr, __file__]):
         _run(["gcc", "-O2", "-std=gnu11", "-fPIC", "-shared", "-fopenmp", "-mfma",
-              "-ffp-contract=off", "-fno-fast-math", "-o", out, src, "-lm"])
+              "-ffp-contract=off", "-fno-fast-math", "-o", out, *srcs, "-lm"])
     return out
 
 

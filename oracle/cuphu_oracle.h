@@ -14,6 +14,8 @@
 #ifndef CUPHU_ORACLE_H
 #define CUPHU_ORACLE_H
 
+#include <stdint.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -75,6 +77,17 @@ int  orc_unwrap_tiled(const float *phase, const float *corr, const unsigned char
 
 double orc_dot_canonical(const double *a, const double *b, int nrow, int ncol,
                          int tx, int vx, int by);
+
+/* cuphu_oracle_post.c: the optional post-passes on a stitched scene */
+void orc_fix_cycle_spikes(float *unw, const unsigned char *mask, int nrow, int ncol);
+void orc_neighbor_feedback(float *unw, const unsigned char *mask, int nrow, int ncol, int ntr,
+                           int ntc, int rovl, int covl, int feather);
+
+/* cuphu_oracle_bridge.c: phase bridging; returns the number of regions
+ * bridged (0 when there was nothing to bridge and nothing was changed) */
+int orc_bridge(float *unw, uint32_t *conncomp, int nrow, int ncol, const unsigned char *mask,
+               int radius, int min_num_pixel, int erosion_size, int max_boundary_samples,
+               int ramp_type, int ramp_max_num_sample);
 
 #ifdef __cplusplus
 }
