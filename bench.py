@@ -136,6 +136,101 @@ def cpu_baseline(ig, g, nlooks, mode, n_irls):
     return n * n / dt / 1e6, dt, int(it.sum()), n
 
 
+def _tile_owner(n, nt, ovl, i):
+    """Tile whose merged output holds row (or column) i: tiles are written in
+    order and each keeps its interior minus half the overlap on inner sides
+    (cuphu_solver.cpp:2002-2031), so the last tile covering i owns it."""
+    import oracle as O
+    own = 0
+    for t in range(nt):
+        f, ln = O.tile_bounds(n, nt, ovl, t)
+        lo = f + (ovl // 2 if t > 0 else 0)
+        hi = f + ln - (ovl // 2 if t < nt - 1 else 0)
+        if lo <= i < hi:
+            own = t
+    return own
+
+
+def flip_details(ph, g, nlooks, mode, flips, ntiles, ovl, n_irls, limit=8):
+    """For pixels whose cycle differs between the mixed and FP64 solves of the
+    tiled scene: the owning tile solved alone in both precisions (each
+    tile's solve does not depend on the rest of the job), and the distance
+    of each continuous solution from the half cycle at which the congruence
+    projection rounds the other way, in cycles."""
+    import torch
+    import oracle as O
+    from cuphu_b200._lib import CuPhuSolveStats, check, default_params, default_solve_options, lib
+    L = lib()
+    nrow, ncol = ph.shape
+    out = []
+    for (r, c) in flips[:limit]:
+        tr, tc = _tile_owner(nrow, ntiles[0], ovl, r), _tile_owner(ncol, ntiles[1], ovl, c)
+        r0, nr = O.tile_bounds(nrow, ntiles[0], ovl, tr)
+        c0, nc = O.tile_bounds(ncol, ntiles[1], ovl, tc)
+        tph = torch.from_numpy(np.ascontiguousarray(ph[r0:r0 + nr, c0:c0 + nc])).cuda()
+        tg = torch.from_numpy(np.ascontiguousarray(g[r0:r0 + nr, c0:c0 + nc])).cuda()
+        narcs = (nr - 1) * nc + nr * (nc - 1)
+        cost = torch.empty((narcs, 4), dtype=torch.int16, device="cuda")
+        pc = default_params(nlooks=nlooks, ncorrlooks=nlooks)
+        check(L.cuphu_build_costs_device(C.c_void_p(tph.data_ptr()), C.c_void_p(tg.data_ptr()),
+                                         None, nr, nc, 1, C.byref(pc), C.c_void_p(cost.data_ptr()),
+                                         None, None))
+        rec = {"pixel": [int(r), int(c)], "tile": [tr, tc]}
+        for name, prec in (("mixed", 0), ("fp64", 1)):
+            du = torch.empty((nr, nc), dtype=torch.float32, device="cuda")
+            dcont = torch.empty((nr, nc), dtype=torch.float32, device="cuda")
+            o = default_solve_options(precision=prec, n_irls=n_irls)
+            st = CuPhuSolveStats()
+            check(L.cuphu_laplace_solve_device(C.c_void_p(cost.data_ptr()), 4,
+                                               C.c_void_p(tph.data_ptr()), nr, nc, C.byref(o),
+                                               C.c_void_p(du.data_ptr()), None,
+                                               C.c_void_p(dcont.data_ptr()), C.byref(st), None))
+            torch.cuda.synchronize()
+            u = float(dcont[r - r0, c - c0].item())
+            d = (u - float(ph[r, c])) / (2 * np.pi)
+            rec[f"cycles_{name}"] = d
+            rec[f"half_cycle_distance_{name}"] = abs(d - np.floor(d) - 0.5)
+        out.append(rec)
+    return out
+
+
+def parity_crop(ig, g, nlooks, mode, n=2880, n_irls=16):
+    """FP64 GPU pipeline (host-buffer entry point, the reference's host
+    phase) against the oracle's restatement of the reference pipeline on an
+    n x n crop of the scene (3 x 3 auto tiles at n = 2880), plus the mixed
+    solve's cycle mismatches against the same oracle."""
+    import oracle as O
+    from cuphu_b200._lib import (check, default_params, default_solve_options,
+                                 default_tile_params, lib, ptr)
+    from cuphu_b200._unwrap import _auto_ntiles_by_target_size
+    L = lib()
+    cig = np.ascontiguousarray(ig[:n, :n])
+    cg = np.ascontiguousarray(g[:n, :n])
+    nt = _auto_ntiles_by_target_size(n, n, 1024, 64, 64)
+    p = default_params(nlooks=nlooks, ncorrlooks=nlooks)
+    t = default_tile_params(ntilerow=nt[0], ntilecol=nt[1], rowovrlp=64, colovrlp=64)
+    got = {}
+    for name, prec in (("fp64", 1), ("mixed", 0)):
+        o = default_solve_options(precision=prec, n_irls=n_irls, ref_row=-1, ref_col=-1)
+        u = np.empty((n, n), np.float32)
+        c = np.empty((n, n), np.uint32)
+        check(L.cuphu_unwrap_ex(ptr(cig.view(np.float32)), ptr(cg), None, None, n, n, mode,
+                                C.byref(p), C.byref(t), C.byref(o), 0, ptr(u), ptr(c), None))
+        got[name] = (u, c)
+    t0 = time.perf_counter()
+    want_u, want_c, _ = O.unwrap_tiled(O.phase_from_igram(cig), cg, nlooks, mode=mode, ntiles=nt,
+                                       overlap=(64, 64), opts=O.lap_opts(n_irls=n_irls))
+    oracle_s = time.perf_counter() - t0
+    u64, c64 = got["fp64"]
+    um = got["mixed"][0]
+    return {"crop": [n, n], "tiles": list(nt), "n_irls": n_irls, "phase": "host atan2f",
+            "fp64_unw_bit_mismatches": int(np.sum(u64.view(np.int32) != want_u.view(np.int32))),
+            "fp64_cycle_mismatches": int(np.sum(np.abs(u64.astype(np.float64) - want_u) > np.pi)),
+            "fp64_conncomp_mismatches": int(np.sum(c64 != want_c)),
+            "mixed_cycle_mismatches": int(np.sum(np.abs(um.astype(np.float64) - want_u) > np.pi)),
+            "oracle_s": oracle_s, "oracle_threads": os.cpu_count()}
+
+
 def adjoint_c4(seed=0, fd_arcs=0, fd_crop=256):
     """The differentiable WLS/IRLS solve on the 2048^2 DEFO configuration
     (5 IRLS passes): forward and backward device time of the mixed solver,
@@ -237,39 +332,28 @@ def adjoint_c4(seed=0, fd_arcs=0, fd_crop=256):
     return out
 
 
-def run_batch(args, rank, world, local_rank):
-    """The 48-interferogram configuration (sides from {512, 1024, 2048,
-    3072}, DEFO, nlooks 5, each scene auto-tiled): 48 individual
-    cuphu_unwrap_device calls, one persistent batched launch
+def _batch_core(data, reps, warm_each, sync_ranks=None):
+    """The three ways of solving a list of scenes on this GPU: one
+    cuphu_unwrap_device call per scene, one persistent batched launch
     (cuphu_unwrap_batch_device) and replays of its CUDA graph
-    (cuphu_batch_graph_*), with the outputs of the three compared."""
+    (cuphu_batch_graph_*).  Returns the device time (CUDA events) and wall
+    time of each per repetition, and whether the outputs are identical."""
     import torch
-    from cuphu_b200 import synthetic as S
     from cuphu_b200._lib import (CuPhuScene, check, default_params, default_solve_options,
                                  default_tile_params, lib)
-    from cuphu_b200.replicas import max_over_ranks, shard_scenes
-    torch.cuda.set_device(local_rank)
     L = lib()
-    data = S.batch_scenes(48, seed=args.seed)
-    total_px = sum(int(g.size) for _, g, _ in data)
-    # N GPUs: the same 48 scenes, split by scene (no data-path collective)
-    mine = shard_scenes([int(g.size) for _, g, _ in data], rank, world)
-    data = [data[i] for i in mine]
     p = default_params(nlooks=5.0, ncorrlooks=5.0)
     o = default_solve_options(precision=0, ref_row=0, ref_col=0)
     stream = torch.cuda.current_stream()
     sptr = C.c_void_p(stream.cuda_stream)
     bufs = []
-    npix = 0
     for ig, g, _ in data:
         nr, nc = g.shape
-        npix += nr * nc
         bufs.append(dict(nr=nr, nc=nc, t=tiles_for(nr, nc),
                          ig=torch.from_numpy(ig.view(np.float32)).cuda(),
                          g=torch.from_numpy(g).cuda(),
                          u=torch.empty((nr, nc), dtype=torch.float32, device="cuda"),
                          c=torch.empty((nr, nc), dtype=torch.int32, device="cuda")))
-    del data
     scenes = (CuPhuScene * len(bufs))()
     for i, b in enumerate(bufs):
         scenes[i] = CuPhuScene(b["ig"].data_ptr(), None, b["g"].data_ptr(), None, None, b["nr"],
@@ -290,8 +374,9 @@ def run_batch(args, rank, world, local_rank):
         check(L.cuphu_unwrap_batch_device(scenes, len(bufs), 1, C.byref(p), C.byref(o), None,
                                           sptr))
 
-    def timed(fn, reps):
-        fn()
+    def timed(fn):
+        if warm_each:
+            fn()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -306,44 +391,96 @@ def run_batch(args, rank, world, local_rank):
     def outputs():
         return [(b["u"].cpu().numpy().copy(), b["c"].cpu().numpy().copy()) for b in bufs]
 
-    if world > 1:
-        import torch.distributed as tdist
-        tdist.barrier()
-    clocks = ClockSampler(local_rank)
-    clocks.start()
-    ms_ind, wall_ind = timed(individual, args.steps)
+    if not warm_each:
+        batched()                       # sizes the workspace once for all three
+    if sync_ranks:
+        sync_ranks()
+    ms_ind, wall_ind = timed(individual)
     out_ind = outputs()
-    ms_bat, wall_bat = timed(batched, args.steps)
+    ms_bat, wall_bat = timed(batched)
     out_bat = outputs()
     graph = C.c_void_p()
     check(L.cuphu_batch_graph_create(scenes, len(bufs), 1, C.byref(p), C.byref(o),
                                      C.byref(graph)))
     try:
-        ms_gr, wall_gr = timed(lambda: check(L.cuphu_batch_graph_launch(graph, sptr)), args.steps)
+        ms_gr, wall_gr = timed(lambda: check(L.cuphu_batch_graph_launch(graph, sptr)))
         out_gr = outputs()
     finally:
         check(L.cuphu_batch_graph_destroy(graph))
-    clk = clocks.stop()
-    ms_ind, ms_bat, ms_gr = (max_over_ranks(x) for x in (ms_ind, ms_bat, ms_gr))
 
     def same(a, b):
         return all(np.array_equal(x[0].view(np.int32), y[0].view(np.int32)) and
                    np.array_equal(x[1], y[1]) for x, y in zip(a, b))
 
+    return {"individual": (ms_ind, wall_ind), "batched": (ms_bat, wall_bat),
+            "graph": (ms_gr, wall_gr),
+            "identical": {"batched_vs_individual": same(out_bat, out_ind),
+                          "graph_vs_batched": same(out_gr, out_bat)},
+            "n_irls": o.n_irls}
+
+
+def batch_c3(seed=0):
+    """The 48-interferogram configuration on this GPU, one repetition of each
+    way of solving it (the key the default bench line carries)."""
+    from cuphu_b200 import synthetic as S
+    data = S.batch_scenes(48, seed=seed)
+    total_px = sum(int(g.size) for _, g, _ in data)
+    r = _batch_core(data, reps=1, warm_each=False)
+    del data
+    mp = total_px / 1e6
+    return {"config": "c3_batch48", "scenes": 48, "pixels": total_px, "cost": "defo",
+            "nlooks": 5.0, "n_irls": r["n_irls"], "precision": "mixed",
+            "individual_calls": {"ms": r["individual"][0], "mpix_s": mp / (r["individual"][0] * 1e-3)},
+            "batched_launch": {"ms": r["batched"][0], "mpix_s": mp / (r["batched"][0] * 1e-3)},
+            "graph_replay": {"ms": r["graph"][0], "mpix_s": mp / (r["graph"][0] * 1e-3)},
+            "speedup_batched_vs_individual": r["individual"][0] / r["batched"][0],
+            "outputs_identical": r["identical"]}
+
+
+def run_batch(args, rank, world, local_rank):
+    """The 48-interferogram configuration (sides from {512, 1024, 2048,
+    3072}, DEFO, nlooks 5, each scene auto-tiled): 48 individual
+    cuphu_unwrap_device calls, one persistent batched launch
+    (cuphu_unwrap_batch_device) and replays of its CUDA graph
+    (cuphu_batch_graph_*), with the outputs of the three compared."""
+    import torch
+    from cuphu_b200 import synthetic as S
+    from cuphu_b200.replicas import max_over_ranks, shard_scenes
+    torch.cuda.set_device(local_rank)
+    data = S.batch_scenes(48, seed=args.seed)
+    total_px = sum(int(g.size) for _, g, _ in data)
+    # N GPUs: the same 48 scenes, split by scene (no data-path collective)
+    mine = shard_scenes([int(g.size) for _, g, _ in data], rank, world)
+    data = [data[i] for i in mine]
+
+    def sync():
+        if world > 1:
+            import torch.distributed as tdist
+            tdist.barrier()
+
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    nloc = len(data)
+    r = _batch_core(data, reps=args.steps, warm_each=True, sync_ranks=sync)
+    del data
+    clk = clocks.stop()
+    (ms_ind, wall_ind), (ms_bat, wall_bat), (ms_gr, wall_gr) = (r["individual"], r["batched"],
+                                                                r["graph"])
+    ms_ind, ms_bat, ms_gr = (max_over_ranks(x) for x in (ms_ind, ms_bat, ms_gr))
+    same_flags = r["identical"]
     mp = total_px / 1e6
     line = {"metric": "Mpix/s unwrapped, 48-interferogram uneven batch (mixed-precision Laplace PCG)",
             "value": mp / (ms_gr * 1e-3), "unit": "Mpix/s", "n_gpus": world,
             "steps": args.steps, "warmup": 1, "ms_per_step": ms_gr, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "c3_batch48", "scenes": 48, "pixels": total_px,
-                       "scenes_per_rank": len(bufs),
-                       "cost": "defo", "nlooks": 5.0, "n_irls": o.n_irls,
+                       "scenes_per_rank": nloc,
+                       "cost": "defo", "nlooks": 5.0, "n_irls": r["n_irls"],
                        "tiles": "auto (target 1024, overlap 64)"},
             "individual_calls": {"ms": ms_ind, "wall_ms": wall_ind, "mpix_s": mp / (ms_ind * 1e-3)},
             "batched_launch": {"ms": ms_bat, "wall_ms": wall_bat, "mpix_s": mp / (ms_bat * 1e-3)},
             "graph_replay": {"ms": ms_gr, "wall_ms": wall_gr, "mpix_s": mp / (ms_gr * 1e-3)},
-            "outputs_identical": {"batched_vs_individual": same(out_bat, out_ind),
-                                  "graph_vs_batched": same(out_gr, out_bat)},
+            "outputs_identical": same_flags,
             "clocks": clk}
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -515,11 +652,23 @@ def run_ours(args, rank, world, local_rank):
         ms64 = ee0.elapsed_time(ee1)
         unw64 = d_u.cpu().numpy()
         diff = unw_mixed.astype(np.float64) - unw64
+        flip = np.abs(diff) > np.pi
+        flips = [tuple(x) for x in np.argwhere(flip)]
+        d_ph = torch.empty((nrow, ncol), dtype=torch.float32, device="cuda")
+        check(L.cuphu_phase_gpu(C.c_void_p(d_ig.data_ptr()), C.c_longlong(npix),
+                                C.c_void_p(d_ph.data_ptr()), sptr))
+        ph_dev = d_ph.cpu().numpy()
+        del d_ph
         result["fp64"] = {"value": npix / (ms64 * 1e-3) / 1e6, "ms_per_step": ms64,
                           "speedup_mixed_vs_fp64": ms64 / ms,
-                          "cycle_mismatches": int(np.sum(np.abs(diff) > np.pi)),
+                          "cycle_mismatches": int(flip.sum()),
                           "rms_rad": float(np.sqrt(np.mean(diff ** 2))),
-                          "pcg_iterations": st64.total_iters}
+                          "rms_rad_outside_flips": float(np.sqrt(np.mean(diff[~flip] ** 2))),
+                          "max_abs_rad_outside_flips": float(np.abs(diff[~flip]).max()),
+                          "pcg_iterations": st64.total_iters,
+                          "mixed_pcg_iterations": st.total_iters,
+                          "flips": flip_details(ph_dev, g, nlooks, mode, flips, (ntr, ntc), 64,
+                                                opts.n_irls)}
 
     # cost-kernel bandwidth (DEFO costs from the wrapped phase, 8192^2)
     if rank == 0:
@@ -553,6 +702,12 @@ def run_ours(args, rank, world, local_rank):
 
     if rank == 0 and not args.skip_adjoint:
         result["adjoint"] = adjoint_c4(args.seed, args.adjoint_fd)
+
+    if rank == 0 and not args.skip_parity:
+        result["parity"] = parity_crop(ig, g, nlooks, mode, n_irls=opts.n_irls)
+
+    if rank == 0 and not args.skip_batch:
+        result["batch"] = batch_c3(args.seed)
 
     # end to end through the C ABI with pinned host buffers
     h_ig = torch.from_numpy(ig.view(np.float32)).pin_memory()
@@ -594,7 +749,9 @@ def run_ours(args, rank, world, local_rank):
                            "precision": args.precision, "parallelism": f"replicas{world}",
                            "l2": "inputs (805 MB) larger than L2", "autotune": tuned},
                 "e2e": {"value": world * npix / e2e_s / 1e6, "unit": "Mpix/s",
-                        "h2d_bytes_per_step": npix * 12, "d2h_bytes_per_step": npix * 8},
+                        "h2d_bytes_per_step": npix * 8, "d2h_bytes_per_step": npix * 8,
+                        "phase": "host atan2f (the reference's), threaded and overlapped "
+                                 "with its upload"},
                 "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
                 "gpu_launches": 14 * args.steps}
         line.update(result)
@@ -614,6 +771,10 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-adjoint", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--skip-parity", action="store_true",
+                    help="skip the FP64-vs-oracle parity check on a 3x3-tile crop")
+    ap.add_argument("--skip-batch", action="store_true",
+                    help="skip the 48-interferogram batch measurement")
     ap.add_argument("--adjoint-fd", type=int, default=0,
                     help="finite-difference check of the adjoint on this many random arcs")
     ap.add_argument("--scale", type=int, default=None,

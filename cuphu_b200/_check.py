@@ -25,10 +25,16 @@ _CHOICES = {
 }
 
 
+def _dtype_of(arr):
+    """dtype without reading a dataset that declares one"""
+    dt = getattr(arr, "dtype", None)
+    return np.dtype(dt) if dt is not None else np.asarray(arr).dtype
+
+
 def _require_dtype(family, arrays):
     accepts, what = _DTYPE_RULES[family]
     for name, arr in arrays.items():
-        dt = np.asarray(arr).dtype
+        dt = _dtype_of(arr)
         if not accepts(dt):
             raise TypeError(f"{name} must be {what}, got dtype={dt}")
 

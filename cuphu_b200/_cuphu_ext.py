@@ -19,9 +19,9 @@ libcuphu_b200 when it is installed as ``cuphu._cuphu_ext``::
 
 Options whose implementation needs SNAPHU's CPU network-flow solver
 (``init='mcf'``/``'mst'``, ``single_tile_reoptimize``) raise
-NotImplementedError, and so do the optional post-passes this build does not
-run (``laplace_neighbor_feedback``, ``fix_cycle_spikes``, ``bridge`` and
-their test hooks): an option is never dropped silently.  Failures of the
+NotImplementedError: an option is never dropped silently.  The post-passes
+``laplace_neighbor_feedback``, ``fix_cycle_spikes`` and ``bridge`` run on the
+device, with their test hooks.  Failures of the
 library raise RuntimeError, as the reference's C++ exceptions surface
 through pybind11.
 """
@@ -145,29 +145,21 @@ def unwrap_arrays(igram, corr, nlooks, cost="smooth", init="mcf", mask=None, mag
     orig_mask = None if orig_mask is None else _array2d(orig_mask, np.uint8, "orig_mask")
     cost_mode = _parse(_COST, cost, _COST_MSG)
     init_meth = _parse(_INIT, init, _INIT_MSG)
-    if bridge_ramp_type is not None and bridge_ramp_type not in _RAMPS:
-        raise ValueError("bridge_ramp_type must be one of: linear, quadratic, linear_range, "
-                         "linear_azimuth, quadratic_range, quadratic_azimuth, or None")
-    for flag, name in ((single_tile_reoptimize, "single_tile_reoptimize"),
-                       (laplace_neighbor_feedback, "laplace_neighbor_feedback"),
-                       (fix_cycle_spikes, "fix_cycle_spikes"), (bridge, "bridge")):
-        if flag:
-            raise NotImplementedError(f"{name} is outside this build")
+    if single_tile_reoptimize:
+        raise NotImplementedError("single_tile_reoptimize is outside this build")
     params = _params(nlooks, costscale, nshortcycle, kperpdpsi, kpardpsi, defomax,
                      min_conncomp_frac, max_ncomps, conncompthresh)
     tile = default_tile_params(ntilerow=int(ntilerow), ntilecol=int(ntilecol),
                                rowovrlp=int(tile_rowovrlp), colovrlp=int(tile_colovrlp),
                                tilecostthresh=int(tilecostthresh),
                                minregionsize=int(minregionsize), nproc=int(nproc),
+                               laplace_neighbor_feedback=int(bool(laplace_neighbor_feedback)),
                                laplace_neighbor_feedback_feather=int(
-                                   laplace_neighbor_feedback_feather))
-    bp = CuPhuBridgeParams()
-    lib().cuphu_default_bridge_params(C.byref(bp))
-    bp.radius, bp.min_num_pixel = int(bridge_radius), int(bridge_min_num_pixel)
-    bp.erosion_size, bp.max_boundary_samples = int(bridge_erosion_size), int(
-        bridge_max_boundary_samples)
-    bp.ramp_type = 0 if bridge_ramp_type is None else 1 + _RAMPS.index(bridge_ramp_type)
-    bp.ramp_max_num_sample = int(bridge_ramp_max_num_sample)
+                                   laplace_neighbor_feedback_feather),
+                               fix_cycle_spikes=int(bool(fix_cycle_spikes)))
+    bp = _bridge_params(bool(bridge), bridge_radius, bridge_min_num_pixel, bridge_erosion_size,
+                        bridge_max_boundary_samples, bridge_ramp_type,
+                        bridge_ramp_max_num_sample)
     res = CuPhuResult()
     rc = lib().cuphu_unwrap(ptr(re), ptr(im), ptr(corr), ptr(mag), ptr(mask), nrow, ncol,
                             cost_mode, init_meth, C.byref(params), C.byref(tile), C.byref(bp),
@@ -227,16 +219,53 @@ def gpu_info(device_id: int = 0) -> dict:
     return _gpu.gpu_info(device_id)
 
 
+def _bridge_params(enabled, radius, min_num_pixel, erosion_size, max_boundary_samples,
+                   ramp_type, ramp_max_num_sample):
+    if ramp_type is not None and ramp_type not in _RAMPS:
+        raise ValueError("bridge_ramp_type must be one of: linear, quadratic, linear_range, "
+                         "linear_azimuth, quadratic_range, quadratic_azimuth, or None")
+    bp = CuPhuBridgeParams()
+    lib().cuphu_default_bridge_params(C.byref(bp))
+    bp.enabled, bp.radius = int(enabled), int(radius)
+    bp.min_num_pixel, bp.erosion_size = int(min_num_pixel), int(erosion_size)
+    bp.max_boundary_samples = int(max_boundary_samples)
+    bp.ramp_type = 0 if ramp_type is None else 1 + _RAMPS.index(ramp_type)
+    bp.ramp_max_num_sample = int(ramp_max_num_sample)
+    return bp
+
+
 def _bridge_apply_test(unw, mask=None, bridge_radius=500, bridge_min_num_pixel=14,
                        bridge_erosion_size=2, bridge_max_boundary_samples=4096,
                        bridge_ramp_type=None, bridge_ramp_max_num_sample=1000000, gpu_id=0):
-    raise NotImplementedError("bridge is outside this build")
+    """Phase bridging on a caller's ``unw``; returns ``(unw, conncomp)``
+    copies (cuphu_py.cu:323-367)."""
+    u = np.array(_array2d(unw, np.float32, "unw"), copy=True)
+    m = None if mask is None else _array2d(mask, np.uint8, "mask")
+    cc = np.zeros(u.shape, np.uint32)
+    bp = _bridge_params(True, bridge_radius, bridge_min_num_pixel, bridge_erosion_size,
+                        bridge_max_boundary_samples, bridge_ramp_type, bridge_ramp_max_num_sample)
+    _call(lib().cuphu_bridge_apply_test(ptr(u), ptr(cc), u.shape[0], u.shape[1], C.byref(bp),
+                                        ptr(m), int(gpu_id)))
+    return u, cc
 
 
 def _laplace_neighbor_feedback_test(unw, mask=None, ntilerow=1, ntilecol=1, row_ovrlp=0,
                                     col_ovrlp=0, feather_px=200):
-    raise NotImplementedError("laplace_neighbor_feedback is outside this build")
+    """The tile-boundary refinement on a caller's stitched ``unw``; returns a
+    refined copy (cuphu_py.cu:360-403)."""
+    u = np.array(_array2d(unw, np.float32, "unw"), copy=True)
+    m = None if mask is None else _array2d(mask, np.uint8, "mask")
+    _call(lib().cuphu_laplace_neighbor_feedback_test(ptr(u), ptr(m), u.shape[0], u.shape[1],
+                                                     int(ntilerow), int(ntilecol),
+                                                     int(row_ovrlp), int(col_ovrlp),
+                                                     int(feather_px)))
+    return u
 
 
 def _fix_cycle_spikes_test(unw, mask=None):
-    raise NotImplementedError("fix_cycle_spikes is outside this build")
+    """The isolated row/column whole-cycle spike correction on a caller's
+    ``unw``; returns a corrected copy (cuphu_py.cu:408-431)."""
+    u = np.array(_array2d(unw, np.float32, "unw"), copy=True)
+    m = None if mask is None else _array2d(mask, np.uint8, "mask")
+    _call(lib().cuphu_fix_cycle_spikes_test(ptr(u), ptr(m), u.shape[0], u.shape[1]))
+    return u

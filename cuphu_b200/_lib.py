@@ -10,7 +10,7 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.environ.get("CUPHU_B200_LIB", os.path.join(HERE, "lib", "libcuphu_b200.so"))
+LIB_PATH = os.path.join(HERE, "lib", "libcuphu_b200.so")
 
 _D, _L, _I = C.c_double, C.c_long, C.c_int
 
@@ -73,7 +73,8 @@ class CuPhuResult(C.Structure):
 class CuPhuSolveOptions(C.Structure):
     _fields_ = [("precision", _I), ("n_irls", _I), ("irls_delta_max", C.c_float),
                 ("irls_delta_min", C.c_float), ("max_iter", _I), ("tol", C.c_float),
-                ("replace_every", _I), ("ref_row", _I), ("ref_col", _I), ("timeout_ms", _I)]
+                ("replace_every", _I), ("ref_row", _I), ("ref_col", _I), ("timeout_ms", _I),
+                ("device_phase", _I), ("merge_conncomp", _I)]
 
 
 class CuPhuSolveStats(C.Structure):
@@ -120,6 +121,18 @@ SIGNATURES = {
                                         P(CuPhuSolveStats), VP]),
     "cuphu_integrate_phase_gpu": (_I, [VP, VP, VP, _I, _I, _I, VP]),
     "cuphu_integrate_phase_noalloc": (_I, [VP, VP, VP, _I, _I, VP, VP]),
+    "cuphu_stream_create": (_I, [_I, _I, _I, _I, P(VP)]),
+    "cuphu_stream_put_rows": (_I, [VP, _I, _I, VP, VP, VP, VP]),
+    "cuphu_stream_unwrap": (_I, [VP, _I, P(CuPhuParams), P(CuPhuTileParams),
+                                 P(CuPhuSolveOptions), P(CuPhuSolveStats)]),
+    "cuphu_stream_get_rows": (_I, [VP, _I, _I, VP, VP]),
+    "cuphu_stream_destroy": (_I, [VP]),
+    "cuphu_mst_costs_device": (_I, [VP, C.c_longlong, _L, _L, VP, VP]),
+    "cuphu_mcf_inputs": (_I, [VP, VP, VP, VP, _I, _I, _I, P(CuPhuParams), _I, VP, VP, VP]),
+    "cuphu_laplace_neighbor_feedback_test": (_I, [VP, VP, _I, _I, _I, _I, _I, _I, _I]),
+    "cuphu_fix_cycle_spikes_test": (_I, [VP, VP, _I, _I]),
+    "cuphu_laplace_neighbor_feedback_device": (_I, [VP, VP, _I, _I, _I, _I, _I, _I, _I, VP]),
+    "cuphu_fix_cycle_spikes_device": (_I, [VP, VP, _I, _I, VP]),
     "cuphu_conncomp_gpu": (_I, [VP, VP, VP, _I, _I, VP, VP, P(CuPhuParams), _I, VP]),
     "cuphu_conncomp_ex": (_I, [VP, VP, VP, _I, _I, C.c_float, _D, _L, _I, VP]),
     "cuphu_incrcost_early_exit": (_I, [VP, VP, _I, _L, _I, VP, VP, VP]),
@@ -134,6 +147,9 @@ SIGNATURES = {
     "cuphu_gpu_count": (_I, []),
     "cuphu_gpu_name": (_I, [_I, C.c_char_p, _I]),
     "cuphu_gpu_info": (_I, [_I, P(C.c_longlong), P(_I), P(_I), P(_I)]),
+    "cuphu_bridge_apply_test": (_I, [VP, VP, _I, _I, P(CuPhuBridgeParams), VP, _I]),
+    "cuphu_bridge_device": (_I, [VP, VP, VP, _I, _I, P(CuPhuBridgeParams), VP]),
+    "cuphu_test_skip_barrier_once": (_I, [_I, _I]),
     "cuphu_last_status": (_I, [_I]),
     "cuphu_release_workspace": (_I, [_I]),
 }

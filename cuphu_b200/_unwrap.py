@@ -2,8 +2,10 @@
 
 Same signature, defaults, validation and output conventions as the reference
 (cuphu/_unwrap.py:167-629); the work runs in libcuphu_b200 through the C ABI
-(``cuphu_unwrap_ex``).  ``init='mcf'`` / ``'mst'`` need SNAPHU's CPU
-network-flow solver and raise NotImplementedError.  New keyword-only options
+(``cuphu_unwrap_ex``), the optional post-passes ``laplace_neighbor_feedback``
+and ``fix_cycle_spikes`` included.  ``init='mcf'`` / ``'mst'`` and
+``single_tile_reoptimize`` need SNAPHU's CPU network-flow solver and raise
+NotImplementedError; ``bridge`` runs the device bridging pass.  New keyword-only options
 (``precision``, ``n_irls``, ``max_iter``, ``tol``, ``stats``) default to the
 reference behaviour.
 """
@@ -23,6 +25,7 @@ from cuphu_b200._check import (
     check_shape_match,
 )
 from cuphu_b200._lib import (
+    CuPhuBridgeParams,
     CuPhuSolveStats,
     check,
     default_params,
@@ -37,6 +40,8 @@ __all__ = ["unwrap"]
 _DEFAULT_LAPLACE_TILE_OVERLAP = 64
 _COST = {"smooth": 0, "defo": 1, "topo": 2}
 _PRECISION = {"mixed": 0, "fp64": 1}
+_RAMPS = (None, "linear", "quadratic", "linear_range", "linear_azimuth", "quadratic_range",
+          "quadratic_azimuth")
 
 
 def _auto_ntiles_by_target_size(nrow, ncol, target_tile_size, row_ovrlp, col_ovrlp):
@@ -51,6 +56,44 @@ def _auto_ntiles_by_target_size(nrow, ncol, target_tile_size, row_ovrlp, col_ovr
     ntilerow = max(1, round(nrow / edge))
     ntilecol = max(1, round(ncol / edge))
     return ntilerow, ntilecol
+
+
+_BAND_BYTES = 64 << 20     # interferogram bytes per streamed band
+
+
+def _streamable(a) -> bool:
+    """A 2-D dataset that is not an in-memory array and can be read by row
+    slices (h5py and zarr datasets, and the like)."""
+    return (not isinstance(a, np.ndarray) and hasattr(a, "__getitem__") and
+            hasattr(a, "dtype") and getattr(a, "ndim", None) == 2)
+
+
+def _unwrap_streamed(igram, corr, solve_mask, orig_mask, nrow, ncol, cost, params, tile, opts,
+                     gpu_id):
+    """Feed the scene to the GPU in row bands (cuphu_stream_*): each band is
+    read from its dataset while the previous one is uploaded."""
+    flags = (1 if solve_mask is not None else 0) | (2 if orig_mask is not None else 0)
+    h = C.c_void_p()
+    check(lib().cuphu_stream_create(nrow, ncol, flags, gpu_id, C.byref(h)))
+    try:
+        band = max(1, _BAND_BYTES // (8 * ncol))
+        for r0 in range(0, nrow, band):
+            r1 = min(nrow, r0 + band)
+            ig = np.ascontiguousarray(igram[r0:r1], dtype=np.complex64)
+            co = np.ascontiguousarray(corr[r0:r1], dtype=np.float32)
+            m = None if solve_mask is None else np.ascontiguousarray(solve_mask[r0:r1])
+            om = None if orig_mask is None else np.ascontiguousarray(orig_mask[r0:r1])
+            check(lib().cuphu_stream_put_rows(h, r0, r1 - r0, ptr(ig.view(np.float32)), ptr(co),
+                                              ptr(m), ptr(om)))
+        st = CuPhuSolveStats()
+        check(lib().cuphu_stream_unwrap(h, cost, C.byref(params), C.byref(tile), C.byref(opts),
+                                        C.byref(st)))
+        unw_out = np.empty((nrow, ncol), dtype=np.float32)
+        cc_out = np.empty((nrow, ncol), dtype=np.uint32)
+        check(lib().cuphu_stream_get_rows(h, 0, nrow, ptr(unw_out), ptr(cc_out)))
+    finally:
+        lib().cuphu_stream_destroy(h)
+    return unw_out, cc_out, st
 
 
 def _dilate_mask(valid: np.ndarray, pixels: int) -> np.ndarray:
@@ -75,7 +118,8 @@ def unwrap(igram, corr, nlooks, cost="smooth", init="mcf", *, mask=None, mask_pa
            bridge_radius=500, bridge_min_num_pixel=14, bridge_erosion_size=2,
            bridge_max_boundary_samples=4096, bridge_ramp_type=None,
            bridge_ramp_max_num_sample=1000000, reference_pixel=(0, 0), gpu_id=0, unw=None,
-           conncomp=None, precision="mixed", n_irls=None, max_iter=None, tol=None, stats=None):
+           conncomp=None, precision="mixed", n_irls=None, max_iter=None, tol=None, stats=None,
+           merge_conncomp=False):
     """Unwrap an interferogram with the weighted-least-squares Laplace solver.
 
     Parameters mirror ``cuphu.unwrap``: ``igram`` complex 2-D, ``corr`` float
@@ -95,16 +139,22 @@ def unwrap(igram, corr, nlooks, cost="smooth", init="mcf", *, mask=None, mask_pa
     override the IRLS pass count (16), PCG iteration cap (1000) and
     tolerance (1e-3) and otherwise honour CUPHU_N_IRLS,
     CUPHU_LAPLACE_MAX_ITER and CUPHU_LAPLACE_TOL like the reference; a dict
-    passed as ``stats`` receives solver statistics.
+    passed as ``stats`` receives solver statistics; ``merge_conncomp=True``
+    labels the whole stitched scene at once, so components that cross tile
+    seams get one label (the reference offsets per-tile labels instead).
 
     Returns ``(unw float32, conncomp uint32)``, written into ``unw`` /
     ``conncomp`` with ``[...]`` when those are given.
     """
-    igram = np.asarray(igram)
-    corr = np.asarray(corr)
-    if igram.ndim != 2:
-        raise ValueError(f"igram must be 2-D, got ndim={igram.ndim}")
-    nrow, ncol = igram.shape
+    # datasets that can be read by row bands (h5py, zarr, ...) stream to the
+    # GPU band by band; everything else is read whole, as the reference does
+    streamed = _streamable(igram) and _streamable(corr)
+    if not streamed:
+        igram = np.asarray(igram)
+        corr = np.asarray(corr)
+    if np.ndim(igram) != 2:
+        raise ValueError(f"igram must be 2-D, got ndim={np.ndim(igram)}")
+    nrow, ncol = np.shape(igram)
     check_shape_match((nrow, ncol), corr=corr)
     if mask is not None:
         mask = np.asarray(mask)
@@ -128,11 +178,11 @@ def unwrap(igram, corr, nlooks, cost="smooth", init="mcf", *, mask=None, mask_pa
         raise NotImplementedError(
             f"init={init!r} runs SNAPHU's CPU network-flow solver, which is outside this "
             "build; use init='laplace'")
-    for flag, name in ((single_tile_reoptimize, "single_tile_reoptimize"),
-                       (laplace_neighbor_feedback, "laplace_neighbor_feedback"),
-                       (fix_cycle_spikes, "fix_cycle_spikes"), (bridge, "bridge")):
-        if flag:
-            raise NotImplementedError(f"{name} is outside this build")
+    if single_tile_reoptimize:
+        raise NotImplementedError("single_tile_reoptimize is outside this build")
+    if bridge_ramp_type is not None and bridge_ramp_type not in _RAMPS:
+        raise ValueError("bridge_ramp_type must be one of: linear, quadratic, linear_range, "
+                         "linear_azimuth, quadratic_range, quadratic_azimuth, or None")
 
     if nproc < 1:
         nproc = os.cpu_count() or 1
@@ -149,20 +199,35 @@ def unwrap(igram, corr, nlooks, cost="smooth", init="mcf", *, mask=None, mask_pa
 
     # Non-finite igram samples read as 0 and non-finite coherence as 0 inside
     # the library, which is what the reference's host-side cleaning produces.
-    igram_c64 = np.ascontiguousarray(igram, dtype=np.complex64)
-    corr_f32 = np.ascontiguousarray(corr, dtype=np.float32)
+    igram_c64 = None if streamed else np.ascontiguousarray(igram, dtype=np.complex64)
+    corr_f32 = None if streamed else np.ascontiguousarray(corr, dtype=np.float32)
     mask_u8 = np.ascontiguousarray(mask, dtype=np.uint8) if mask is not None else None
     solve_mask_u8 = mask_u8
     if mask_u8 is not None and mask_pad_distance > 0:
         solve_mask_u8 = _dilate_mask(mask_u8 != 0, int(mask_pad_distance)).astype(np.uint8)
+
+    # With a grown solve mask the boundary refinement must trust only the
+    # original mask's pixels: solve without it, then refine on the stitched
+    # result with the original mask (reference _unwrap.py:539-598).
+    feedback_needs_orig_mask = (mask_u8 is not None and mask_pad_distance > 0
+                                and bool(laplace_neighbor_feedback))
+    internal_feedback = bool(laplace_neighbor_feedback) and not feedback_needs_orig_mask
+    # bridging and that refinement follow the library's pipeline here, so the
+    # reference-pixel shift follows them too (as in the reference's Python)
+    shift_here = feedback_needs_orig_mask or bool(bridge)
 
     kperp, kpar = int(phase_grad_window[0]), int(phase_grad_window[1])
     params = default_params(nlooks=float(nlooks), ncorrlooks=float(nlooks), kperpdpsi=kperp,
                             kpardpsi=kpar, minconncompfrac=float(min_conncomp_frac))
     tile = default_tile_params(ntilerow=ntilerow, ntilecol=ntilecol, rowovrlp=row_ovrlp,
                                colovrlp=col_ovrlp, tilecostthresh=int(tile_cost_thresh),
-                               minregionsize=int(min_region_size), nproc=int(nproc))
-    opts = default_solve_options(precision=_PRECISION[precision])
+                               minregionsize=int(min_region_size), nproc=int(nproc),
+                               laplace_neighbor_feedback=int(internal_feedback),
+                               laplace_neighbor_feedback_feather=int(
+                                   laplace_neighbor_feedback_feather),
+                               fix_cycle_spikes=int(bool(fix_cycle_spikes)))
+    opts = default_solve_options(precision=_PRECISION[precision],
+                                 merge_conncomp=int(bool(merge_conncomp)))
     if n_irls is not None:
         opts.n_irls = int(n_irls)
     if max_iter is not None:
@@ -173,19 +238,50 @@ def unwrap(igram, corr, nlooks, cost="smooth", init="mcf", *, mask=None, mask_pa
         rp, rc = int(reference_pixel[0]), int(reference_pixel[1])
         if not (0 <= rp < nrow and 0 <= rc < ncol):
             raise IndexError(f"reference_pixel {reference_pixel} outside {nrow}x{ncol}")
-        opts.ref_row, opts.ref_col = rp, rc
+        if not shift_here:
+            opts.ref_row, opts.ref_col = rp, rc
 
-    unw_out = np.empty((nrow, ncol), dtype=np.float32)
-    cc_out = np.empty((nrow, ncol), dtype=np.uint32)
-    st = CuPhuSolveStats()
-    check(lib().cuphu_unwrap_ex(ptr(igram_c64.view(np.float32)), ptr(corr_f32),
-                                ptr(solve_mask_u8), ptr(mask_u8), nrow, ncol, _COST[cost],
-                                C.byref(params), C.byref(tile), C.byref(opts), int(gpu_id),
-                                ptr(unw_out), ptr(cc_out), C.byref(st)))
+    if streamed:
+        unw_out, cc_out, st = _unwrap_streamed(igram, corr, solve_mask_u8, mask_u8, nrow, ncol,
+                                               _COST[cost], params, tile, opts, int(gpu_id))
+    else:
+        unw_out = np.empty((nrow, ncol), dtype=np.float32)
+        cc_out = np.empty((nrow, ncol), dtype=np.uint32)
+        st = CuPhuSolveStats()
+        check(lib().cuphu_unwrap_ex(ptr(igram_c64.view(np.float32)), ptr(corr_f32),
+                                    ptr(solve_mask_u8), ptr(mask_u8), nrow, ncol, _COST[cost],
+                                    C.byref(params), C.byref(tile), C.byref(opts), int(gpu_id),
+                                    ptr(unw_out), ptr(cc_out), C.byref(st)))
     if stats is not None:
         stats.update(ntiles=st.ntiles, total_iters=st.total_iters,
                      max_iters_pass=st.max_iters_pass, solve_ms=st.solve_ms,
                      total_ms=st.total_ms, tiles=(ntilerow, ntilecol))
+
+    if bridge:
+        bp = CuPhuBridgeParams()
+        lib().cuphu_default_bridge_params(C.byref(bp))
+        bp.enabled, bp.radius = 1, int(bridge_radius)
+        bp.min_num_pixel, bp.erosion_size = int(bridge_min_num_pixel), int(bridge_erosion_size)
+        bp.max_boundary_samples = int(bridge_max_boundary_samples)
+        bp.ramp_type = _RAMPS.index(bridge_ramp_type)
+        bp.ramp_max_num_sample = int(bridge_ramp_max_num_sample)
+        check(lib().cuphu_bridge_apply_test(ptr(unw_out), ptr(cc_out), nrow, ncol, C.byref(bp),
+                                            ptr(solve_mask_u8), int(gpu_id)))
+    if feedback_needs_orig_mask:
+        check(lib().cuphu_laplace_neighbor_feedback_test(
+            ptr(unw_out), ptr(mask_u8), nrow, ncol, ntilerow, ntilecol, row_ovrlp, col_ovrlp,
+            int(laplace_neighbor_feedback_feather)))
+    if shift_here and reference_pixel is not None:
+        # _unwrap.py:605-617: whole cycles so the reference pixel equals its
+        # wrapped phase
+        ref_val = (np.complex64(np.asarray(igram[rp:rp + 1, rc:rc + 1])[0, 0]) if streamed
+                   else igram_c64[rp, rc])
+        ref_phase = float(np.angle(ref_val))
+        if ref_phase < 0.0:
+            ref_phase += 2.0 * np.pi
+        k = round((float(unw_out[rp, rc]) - ref_phase) / (2.0 * np.pi))
+        if k != 0:
+            unw_out = unw_out - np.float32(k * 2.0 * np.pi)
 
     if mask_u8 is not None and mask_pad_distance > 0:
         cc_out = np.where(mask_u8 != 0, cc_out, 0).astype(cc_out.dtype)

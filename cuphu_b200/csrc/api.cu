@@ -190,7 +190,22 @@ struct SceneIn {
     float *unw = nullptr;
     uint32_t *cc = nullptr;
     int ref_row = -1, ref_col = -1;
+    /* optional post-passes on the stitched scene (multi-tile scenes only,
+     * as in the reference's tiled path, cuphu_solver.cpp:2036-2095) */
+    int feedback = 0, feather = 200, spikes = 0;
+    /* labels of the whole stitched scene instead of per-tile label spaces */
+    int merge_cc = 0;
 };
+
+static bool merges_labels(const SceneIn &in)
+{
+    return in.merge_cc && in.cc && (in.ntr > 1 || in.ntc > 1);
+}
+
+static bool has_postpass(const SceneIn &in)
+{
+    return (in.ntr > 1 || in.ntc > 1) && (in.feedback || in.spikes);
+}
 
 static void tile_bounds(int n, int nt, int ovl, int t, int &first, int &len)
 {
@@ -231,8 +246,9 @@ static int plan_job(const std::vector<SceneIn> &S, const CuPhuParams &prm, Plan 
         sp.covl = in.covl;
         sp.tile0 = (int)pl.tiles.size();
         sp.pair0 = (int)pl.pairs.size();
-        sp.ref_row = in.ref_row;
-        sp.ref_col = in.ref_col;
+        /* with post-passes the reference-pixel shift follows them */
+        sp.ref_row = has_postpass(in) ? -1 : in.ref_row;
+        sp.ref_col = has_postpass(in) ? -1 : in.ref_col;
         sp.maxncomps = (int)std::min<long>(prm.maxncomps, 0x7fffffffL);
         sp.minfrac = prm.minconncompfrac;
         sp.single = single ? 1 : 0;
@@ -414,6 +430,26 @@ static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpt
     const size_t np = (size_t)pl.nplane;
 
     /* device layout */
+    size_t post_bytes = 0;
+    for (auto &in : S)
+        if (has_postpass(in)) post_bytes = std::max(post_bytes, postpass_scratch_bytes(in.nrow, in.ncol));
+    char *d_post = nullptr;
+    SceneOut *d_shift = nullptr;
+    /* scene-level labelling of merged scenes: one descriptor each (uploaded
+     * with the tile descriptors) and one set of pitched planes */
+    int n_merge = 0;
+    size_t cc_bytes = 0;
+    for (auto &in : S)
+        if (merges_labels(in)) {
+            ++n_merge;
+            const size_t pitch = ((size_t)in.ncol + 3) & ~(size_t)3;
+            const size_t items = (size_t)((in.ncol + kItemBx - 1) / kItemBx) *
+                                 ((in.nrow + kItemBy - 1) / kItemBy);
+            cc_bytes = std::max(cc_bytes, (size_t)in.nrow * pitch * 12 + items * 4 +
+                                              (size_t)in.nrow * 8 + 4096);
+        }
+    TileDesc *d_cctd = nullptr;
+    char *d_ccbuf = nullptr;
     size_t need_phase = 0;
     for (auto &in : S)
         if (!in.ph_in) need_phase += (size_t)in.nrow * in.ncol;
@@ -435,6 +471,7 @@ static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpt
         P.q = b.take<char>(np * vs);
         P.diag = b.take<char>(np * vs);
         P.z = b.take<char>(np * vs);
+        P.q1 = jo.fp64 ? nullptr : b.take<float>(np);
         P.unw = b.take<float>(np);
         P.cyc = jo.want_cyc ? b.take<int32_t>(np) : nullptr;
         P.cont = jo.cont_out ? b.take<float>(np) : nullptr;
@@ -457,12 +494,17 @@ static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpt
         d_coff = b.take<unsigned>(ntiles);
         d_sout = b.take<SceneOut>(nsc);
         d_k = b.take<CostConsts>(nsc);
+        d_cctd = b.take<TileDesc>(std::max(n_merge, 1));
         d_st = b.take<TileState>(2 * (size_t)ntiles);
-        /* item partials x2, published tile totals x2, tile item tickets */
-        d_part = b.take<double>(2 * (size_t)pl.nitems + 3 * (size_t)ntiles);
+        /* item partials x2, published tile totals x2 (kNComp components
+         * each), tile item tickets */
+        d_part = b.take<double>(2 * (size_t)kNComp * pl.nitems + (2 * (size_t)kNComp + 1) * ntiles);
         d_ctl = b.take<SolverCtl>(1);
         d_deltas = b.take<float>(o.n_irls + 1);
         d_pass = b.take<int>(o.n_irls + 1);
+        d_post = post_bytes ? b.take<char>(post_bytes) : nullptr;
+        d_shift = b.take<SceneOut>(nsc);
+        d_ccbuf = cc_bytes ? b.take<char>(cc_bytes) : nullptr;
     };
     SolverPlanes P = {};
     float *phase = nullptr, *d_deltas = nullptr;
@@ -534,6 +576,22 @@ static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpt
     put(d_maps, pl.maps.data(), pl.maps.size() * sizeof(int));
     put(d_rowcnt + pl.total_rows, pl.row_tile.data(), pl.total_rows * sizeof(int));
     put(d_k, pl.consts.data(), nsc * sizeof(CostConsts));
+    std::vector<TileDesc> cctd;
+    for (auto &in : S)
+        if (merges_labels(in)) {
+            TileDesc T = {};
+            T.ph = in.unw;
+            T.corr = in.corr;
+            T.mask = in.mask;
+            T.ph_pitch = in.ncol;
+            T.nr = in.nrow;
+            T.nc = in.ncol;
+            T.pitch = (in.ncol + 3) & ~3;
+            T.nbx = (in.ncol + kItemBx - 1) / kItemBx;
+            T.nitems = T.nbx * ((in.nrow + kItemBy - 1) / kItemBy);
+            cctd.push_back(T);
+        }
+    put(d_cctd, cctd.data(), cctd.size() * sizeof(TileDesc));
 
     Timers tm(stats ? 4 : 0);
     cudaEvent_t e0 = tm.e[0], e1 = tm.e[1], e2 = tm.e[2], e3 = tm.e[3];
@@ -558,8 +616,9 @@ static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpt
     }
     CUPHU_TRY_CUDA(cudaMemsetAsync(d_st, 0, 2 * ntiles * sizeof(TileState), s));
     CUPHU_TRY_CUDA(cudaMemsetAsync(d_ctl, 0, sizeof(SolverCtl), s));
-    CUPHU_TRY_CUDA(cudaMemsetAsync(d_part + 2 * (size_t)pl.nitems + 2 * (size_t)ntiles, 0,
-                                   (size_t)ntiles * sizeof(double), s));
+    CUPHU_TRY_CUDA(cudaMemsetAsync(d_part + 2 * (size_t)kNComp * pl.nitems +
+                                       2 * (size_t)kNComp * ntiles,
+                                   0, (size_t)ntiles * sizeof(double), s));
 
     if (jo.wls) return wls_job(pl, P, jo, s, d_tiles, d_item, ntiles, d_st, d_part, d_ctl,
                                d_deltas, d_pass, dev, W, stats);
@@ -609,6 +668,52 @@ static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpt
     if (rc) return rc;
     rc = launch_merge(d_sc, pl.scenes.data(), nsc, d_tiles, P, d_tilek, d_coff, d_sout, s);
     if (rc) return rc;
+    /* post-passes on the stitched scenes, in the reference's order, then the
+     * reference-pixel shift they deferred */
+    for (int i = 0; i < nsc; ++i) {
+        const SceneIn &in = S[i];
+        if (!has_postpass(in)) continue;
+        if (in.feedback)
+            rc = launch_neighbor_feedback(in.unw, in.mask, in.nrow, in.ncol, in.ntr, in.ntc,
+                                          in.rovl, in.covl, in.feather, d_post, s);
+        if (!rc && in.spikes) rc = launch_fix_cycle_spikes(in.unw, in.mask, in.nrow, in.ncol, d_post, s);
+        if (!rc) rc = launch_ref_shift(in.unw, scene_ph[i], in.nrow, in.ncol, in.ref_row, in.ref_col,
+                                       d_shift + i, s);
+        if (rc) return rc;
+    }
+    /* labels over the whole stitched scene (the same criteria as the
+     * per-tile labelling, cuphu_conncomp.cu:290-428): components that cross
+     * tile seams get one label */
+    for (int i = 0, j = 0; i < nsc; ++i) {
+        const SceneIn &in = S[i];
+        if (!merges_labels(in)) continue;
+        const TileDesc &T = cctd[j];
+        const size_t np_s = (size_t)in.nrow * T.pitch;
+        Bump cb(d_ccbuf);
+        SolverPlanes Q = {};
+        Q.unw = cb.take<float>(np_s);
+        Q.cc = cb.take<uint32_t>(np_s);
+        Q.aux = cb.take<uint32_t>(np_s);
+        int *c_item = cb.take<int>(T.nitems);
+        int *c_row = cb.take<int>(2 * (size_t)in.nrow);
+        int *c_nlab = cb.take<int>(1);
+        CUPHU_TRY_CUDA(cudaMemsetAsync(c_item, 0, (size_t)T.nitems * 4, s));
+        CUPHU_TRY_CUDA(cudaMemsetAsync(c_row + in.nrow, 0, (size_t)in.nrow * 4, s));
+        CUPHU_TRY_CUDA(cudaMemcpy2DAsync(Q.unw, (size_t)T.pitch * 4, in.unw, (size_t)in.ncol * 4,
+                                         (size_t)in.ncol * 4, in.nrow, cudaMemcpyDeviceToDevice, s));
+        CcArgs ca;
+        ca.poscost = nullptr;
+        ca.negcost = nullptr;
+        ca.corr_thresh = 0.05f;
+        ca.conncompthresh = prm.conncompthresh;
+        ca.minfrac = prm.minconncompfrac;
+        ca.maxncomps = (int)std::min<long>(prm.maxncomps, 0x7fffffffL);
+        rc = launch_conncomp(d_cctd + j, 1, in.nrow, c_item, T.nitems, Q, ca, c_row, c_nlab, s);
+        if (rc) return rc;
+        CUPHU_TRY_CUDA(cudaMemcpy2DAsync(in.cc, (size_t)in.ncol * 4, Q.cc, (size_t)T.pitch * 4,
+                                         (size_t)in.ncol * 4, in.nrow, cudaMemcpyDeviceToDevice, s));
+        ++j;
+    }
     if (jo.cycles_out && nsc == 1 && ntiles == 1 && P.cyc) {
         const TileDesc &T = pl.tiles[0];
         CUPHU_TRY_CUDA(cudaMemcpy2DAsync(jo.cycles_out, (size_t)T.nc * 4, P.cyc, (size_t)T.pitch * 4,
@@ -654,6 +759,8 @@ static void default_solve_options(CuPhuSolveOptions *o)
     o->ref_row = -1;
     o->ref_col = -1;
     o->timeout_ms = 5000;
+    o->device_phase = 0;
+    o->merge_conncomp = 0;
     if (const char *e = std::getenv("CUPHU_N_IRLS")) o->n_irls = std::atoi(e);
     if (const char *e = std::getenv("CUPHU_IRLS_DELTA_MAX")) o->irls_delta_max = (float)std::atof(e);
     if (const char *e = std::getenv("CUPHU_IRLS_DELTA_MIN")) o->irls_delta_min = (float)std::atof(e);
@@ -676,9 +783,17 @@ static int check_tile_flags(const CuPhuTileParams *t)
     if (t->single_tile_reoptimize)
         return fail(CUPHU_ERR_UNSUPPORTED,
                     "single_tile_reoptimize needs SNAPHU's CPU TreeSolve, which is outside this build");
-    if (t->laplace_neighbor_feedback)
-        return fail(CUPHU_ERR_UNSUPPORTED, "laplace_neighbor_feedback is outside this build");
-    if (t->fix_cycle_spikes) return fail(CUPHU_ERR_UNSUPPORTED, "fix_cycle_spikes is outside this build");
+    if (t->laplace_neighbor_feedback && t->laplace_neighbor_feedback_feather < 0)
+        return fail(CUPHU_ERR_INVALID, "laplace_neighbor_feedback_feather must be >= 0");
+    return 0;
+}
+
+static int check_bridge(const CuPhuBridgeParams *bp)
+{
+    if (!bp) return fail(CUPHU_ERR_INVALID, "bridge params must not be NULL");
+    if (bp->radius < 0 || bp->erosion_size < 0 || bp->max_boundary_samples < 1 ||
+        (int)bp->ramp_type < 0 || (int)bp->ramp_type > 6)
+        return fail(CUPHU_ERR_INVALID, "bad bridge params");
     return 0;
 }
 
@@ -753,6 +868,7 @@ void cuphu_default_params(CuPhuParams *p)
     p->kpardpsi = 7;
     p->defomax = 1.2;
     p->p = -1.0;
+    p->maxcost = 1000.0;
     p->minconncompfrac = 0.01;
     p->conncompthresh = 300;
     p->maxncomps = 32;
@@ -808,12 +924,16 @@ int cuphu_unwrap_device(const float *igram_c64, const float *phase_in, const flo
     if (tile) {
         in.ntr = tile->ntilerow; in.ntc = tile->ntilecol;
         in.rovl = tile->rowovrlp; in.covl = tile->colovrlp;
+        in.feedback = tile->laplace_neighbor_feedback ? 1 : 0;
+        in.feather = tile->laplace_neighbor_feedback_feather;
+        in.spikes = tile->fix_cycle_spikes ? 1 : 0;
     }
     in.nlooks = params->ncorrlooks;
     in.unw = unw_out;
     in.cc = conncomp_out;
     in.ref_row = so.ref_row;
     in.ref_col = so.ref_col;
+    in.merge_cc = so.merge_conncomp ? 1 : 0;
     std::vector<SceneIn> S(1, in);
     JobOpts jo;
     jo.fp64 = so.precision == CUPHU_PREC_FP64;
@@ -1017,7 +1137,10 @@ int cuphu_unwrap_ex(const float *igram_c64, const float *corr, const unsigned ch
     CUPHU_TRY_CUDA(cudaSetDevice(gpu_id));
     cudaStream_t s = lib_stream(gpu_id);
     size_t n = (size_t)nrow * ncol;
-    float *d_ig = dev_alloc_async<float>(2 * n, s), *d_corr = dev_alloc_async<float>(n, s);
+    /* the wrapped phase: the reference's host atan2 (default), or the
+     * interferogram itself for the device's phase kernel */
+    const bool dev_phase = opts && opts->device_phase;
+    float *d_ig = dev_alloc_async<float>(dev_phase ? 2 * n : n, s), *d_corr = dev_alloc_async<float>(n, s);
     float *d_unw = dev_alloc_async<float>(n, s);
     uint32_t *d_cc = dev_alloc_async<uint32_t>(n, s);
     unsigned char *d_mask = mask ? dev_alloc_async<unsigned char>(n, s) : nullptr;
@@ -1026,15 +1149,17 @@ int cuphu_unwrap_ex(const float *igram_c64, const float *corr, const unsigned ch
     if (!d_ig || !d_corr || !d_unw || !d_cc || (mask && !d_mask) || (orig_mask && !d_om))
         rc = fail(CUPHU_ERR_ALLOC, "device allocation failed");
     if (!rc) {
-        rc = copy_async(d_ig, igram_c64, 8 * n, cudaMemcpyHostToDevice, s, "H2D igram");
+        rc = dev_phase ? copy_async(d_ig, igram_c64, 8 * n, cudaMemcpyHostToDevice, s, "H2D igram")
+                       : upload_host_phase(igram_c64, nullptr, nullptr, n, d_ig, gpu_id, s);
         if (!rc) rc = copy_async(d_corr, corr, 4 * n, cudaMemcpyHostToDevice, s, "H2D corr");
         if (!rc && mask) rc = copy_async(d_mask, mask, n, cudaMemcpyHostToDevice, s, "H2D mask");
         if (!rc && orig_mask)
             rc = copy_async(d_om, orig_mask, n, cudaMemcpyHostToDevice, s, "H2D orig_mask");
     }
     if (!rc) {
-        rc = cuphu_unwrap_device(d_ig, nullptr, d_corr, d_mask, d_om, nrow, ncol, cost_mode, params,
-                                 tile, opts, d_unw, d_cc, nullptr, stats, s);
+        rc = cuphu_unwrap_device(dev_phase ? d_ig : nullptr, dev_phase ? nullptr : d_ig, d_corr,
+                                 d_mask, d_om, nrow, ncol, cost_mode, params, tile, opts, d_unw,
+                                 d_cc, nullptr, stats, s);
     }
     if (!rc) rc = copy_async(unw_out, d_unw, 4 * n, cudaMemcpyDeviceToHost, s, "D2H unw");
     if (!rc) rc = copy_async(conncomp_out, d_cc, 4 * n, cudaMemcpyDeviceToHost, s, "D2H conncomp");
@@ -1063,8 +1188,10 @@ int cuphu_unwrap(const float *igram_r, const float *igram_i, const float *corr, 
         return fail(CUPHU_ERR_UNSUPPORTED,
                     "init 'mst'/'mcf' needs SNAPHU's CPU network-flow solver, which is outside this "
                     "build; use init 'laplace'");
-    if (bridge && bridge->enabled)
-        return fail(CUPHU_ERR_UNSUPPORTED, "phase bridging is outside this build");
+    if (bridge && bridge->enabled) {
+        int rb = check_bridge(bridge);
+        if (rb) return rb;
+    }
     if (!igram_r || !igram_i || !corr) return fail(CUPHU_ERR_INVALID, "igram and corr must not be NULL");
     if (nrow < 1 || ncol < 1) return fail(CUPHU_ERR_INVALID, "nrow and ncol must be >= 1");
     int rc = check_common(cost_mode, params);
@@ -1082,23 +1209,20 @@ int cuphu_unwrap(const float *igram_r, const float *igram_i, const float *corr, 
     }
     CUPHU_TRY_CUDA(cudaSetDevice(gpu_id));
     cudaStream_t s = lib_stream(gpu_id);
-    float *d_re = dev_alloc_async<float>(n, s), *d_im = dev_alloc_async<float>(n, s);
     float *d_corr = dev_alloc_async<float>(n, s), *d_unw = dev_alloc_async<float>(n, s);
     float *d_ph = dev_alloc_async<float>(n, s);
     uint32_t *d_cc = dev_alloc_async<uint32_t>(n, s);
     unsigned char *d_mask = mask ? dev_alloc_async<unsigned char>(n, s) : nullptr;
     unsigned char *d_om = orig_mask ? dev_alloc_async<unsigned char>(n, s) : nullptr;
-    if (!d_re || !d_im || !d_corr || !d_unw || !d_ph || !d_cc || (mask && !d_mask) ||
-        (orig_mask && !d_om))
+    if (!d_corr || !d_unw || !d_ph || !d_cc || (mask && !d_mask) || (orig_mask && !d_om))
         rc = fail(CUPHU_ERR_ALLOC, "device allocation failed");
     if (!rc) {
-        rc = copy_async(d_re, igram_r, 4 * n, cudaMemcpyHostToDevice, s, "H2D igram_r");
-        if (!rc) rc = copy_async(d_im, igram_i, 4 * n, cudaMemcpyHostToDevice, s, "H2D igram_i");
+        /* the phase as the reference takes it: host atan2 (cuphu_solver.cpp:1706-1712) */
+        rc = upload_host_phase(nullptr, igram_r, igram_i, n, d_ph, gpu_id, s);
         if (!rc) rc = copy_async(d_corr, corr, 4 * n, cudaMemcpyHostToDevice, s, "H2D corr");
         if (!rc && mask) rc = copy_async(d_mask, mask, n, cudaMemcpyHostToDevice, s, "H2D mask");
         if (!rc && orig_mask)
             rc = copy_async(d_om, orig_mask, n, cudaMemcpyHostToDevice, s, "H2D orig_mask");
-        if (!rc) rc = launch_phase_split(d_re, d_im, d_ph, (long long)n, s);
     }
     if (!rc) {
         CuPhuSolveOptions so;
@@ -1106,18 +1230,196 @@ int cuphu_unwrap(const float *igram_r, const float *igram_i, const float *corr, 
         CuPhuParams p = *params;
         rc = cuphu_unwrap_device(nullptr, d_ph, d_corr, d_mask, d_om, nrow, ncol, cost_mode, &p,
                                  tile, &so, d_unw, d_cc, nullptr, nullptr, s);
+        /* the reference's last stage: bridging over the solve mask
+         * (cuphu_solver.cpp:1720-1722, 2097-2098) */
+        if (!rc && bridge && bridge->enabled)
+            rc = run_bridge(d_unw, d_cc, d_mask, nrow, ncol, *bridge, s);
     }
     if (!rc) rc = copy_async(result->unw, d_unw, 4 * n, cudaMemcpyDeviceToHost, s, "D2H unw");
     if (!rc)
         rc = copy_async(result->conncomp, d_cc, 4 * n, cudaMemcpyDeviceToHost, s, "D2H conncomp");
     cudaError_t e = cudaStreamSynchronize(s);
-    cudaFreeAsync(d_re, s); cudaFreeAsync(d_im, s); cudaFreeAsync(d_corr, s);
+    cudaFreeAsync(d_corr, s);
     cudaFreeAsync(d_unw, s); cudaFreeAsync(d_ph, s); cudaFreeAsync(d_cc, s);
     if (d_mask) cudaFreeAsync(d_mask, s);
     if (d_om) cudaFreeAsync(d_om, s);
     if (!rc && e != cudaSuccess) rc = cuda_fail(e, "cuphu_unwrap");
     if (!rc) rc = device_status(gpu_id);
     return rc;
+}
+
+/* ── phase bridging (ref cuphu_solver.cpp:996-1352) ───────────────────── */
+int cuphu_bridge_device(float *d_unw, uint32_t *d_conncomp, const unsigned char *d_mask, int nrow,
+                        int ncol, const CuPhuBridgeParams *bp, void *stream)
+{
+    int rc = check_bridge(bp);
+    if (rc) return rc;
+    if (!d_unw || !d_conncomp || nrow < 1 || ncol < 1) return fail(CUPHU_ERR_INVALID, "bad arguments");
+    return run_bridge(d_unw, d_conncomp, d_mask, nrow, ncol, *bp, (cudaStream_t)stream);
+}
+
+int cuphu_bridge_apply_test(float *unw, uint32_t *conncomp, int nrow, int ncol,
+                            const CuPhuBridgeParams *bridge, const unsigned char *mask, int gpu_id)
+{
+    int rc = check_bridge(bridge);
+    if (rc) return rc;
+    if (!unw || !conncomp || nrow < 1 || ncol < 1) return fail(CUPHU_ERR_INVALID, "bad arguments");
+    CUPHU_TRY_CUDA(cudaSetDevice(gpu_id));
+    cudaStream_t s = lib_stream(gpu_id);
+    const size_t n = (size_t)nrow * ncol;
+    float *d_u = dev_alloc_async<float>(n, s);
+    uint32_t *d_c = dev_alloc_async<uint32_t>(n, s);
+    unsigned char *d_m = mask ? dev_alloc_async<unsigned char>(n, s) : nullptr;
+    if (!d_u || !d_c || (mask && !d_m)) rc = fail(CUPHU_ERR_ALLOC, "device allocation failed");
+    if (!rc) rc = copy_async(d_u, unw, 4 * n, cudaMemcpyHostToDevice, s, "H2D unw");
+    if (!rc) rc = copy_async(d_c, conncomp, 4 * n, cudaMemcpyHostToDevice, s, "H2D conncomp");
+    if (!rc && mask) rc = copy_async(d_m, mask, n, cudaMemcpyHostToDevice, s, "H2D mask");
+    if (!rc) rc = run_bridge(d_u, d_c, d_m, nrow, ncol, *bridge, s);
+    if (!rc) rc = copy_async(unw, d_u, 4 * n, cudaMemcpyDeviceToHost, s, "D2H unw");
+    if (!rc) rc = copy_async(conncomp, d_c, 4 * n, cudaMemcpyDeviceToHost, s, "D2H conncomp");
+    cudaError_t e = cudaStreamSynchronize(s);
+    for (void *p : {(void *)d_u, (void *)d_c, (void *)d_m})
+        if (p) cudaFreeAsync(p, s);
+    cudaStreamSynchronize(s);
+    if (!rc && e != cudaSuccess) rc = cuda_fail(e, "bridging");
+    return rc;
+}
+
+/* ── failure test of the bounded device waits ─────────────────────────── */
+int cuphu_test_skip_barrier_once(int gpu_id, int block)
+{
+    if (gpu_id < 0 || gpu_id >= 64 || block < 0)
+        return fail(CUPHU_ERR_INVALID, "bad arguments");
+    solver_skip_barrier_once(gpu_id, block);
+    return 0;
+}
+
+/* ── network-flow front-end inputs (the §8(f) GPU-side MCF inputs) ────── */
+int cuphu_mst_costs_device(const void *d_smooth_costs, long long narcs, long nshortcycle,
+                           long maxcost, short *d_out, void *stream)
+{
+    if (!d_smooth_costs || !d_out || narcs < 0 || nshortcycle < 1 || maxcost < 1)
+        return fail(CUPHU_ERR_INVALID, "bad arguments");
+    return launch_mst_costs(static_cast<const short *>(d_smooth_costs), narcs, nshortcycle,
+                            maxcost, d_out, (cudaStream_t)stream);
+}
+
+int cuphu_mcf_inputs(const float *igram_r, const float *igram_i, const float *corr,
+                     const short *weights, int nrow, int ncol, CuPhuCostMode cost_mode,
+                     const CuPhuParams *params, int gpu_id, short *costs_out,
+                     short *mst_costs_out, signed char *residues_out)
+{
+    int rc = check_common(cost_mode, params);
+    if (rc) return rc;
+    if (!igram_r || !igram_i || !corr || !costs_out || nrow < 2 || ncol < 2)
+        return fail(CUPHU_ERR_INVALID, "bad arguments");
+    if (mst_costs_out && cost_mode != CUPHU_COST_SMOOTH)
+        return fail(CUPHU_ERR_UNSUPPORTED,
+                    "initial-flow weights of DEFO/TOPO costs need SNAPHU's CalcCostDefo, which "
+                    "is outside this build");
+    if (mst_costs_out && !(params->maxcost >= 1.0))
+        return fail(CUPHU_ERR_INVALID, "params->maxcost must be >= 1");
+    CUPHU_TRY_CUDA(cudaSetDevice(gpu_id));
+    cudaStream_t s = lib_stream(gpu_id);
+    const size_t n = (size_t)nrow * ncol;
+    const size_t narcs = (size_t)(nrow - 1) * ncol + (size_t)nrow * (ncol - 1);
+    const size_t es = cost_mode == CUPHU_COST_SMOOTH ? 4 : 8;
+    const size_t nres = (size_t)(nrow - 1) * (ncol - 1);
+    float *d_ph = dev_alloc_async<float>(n, s), *d_corr = dev_alloc_async<float>(n, s);
+    short *d_w = weights ? dev_alloc_async<short>(narcs, s) : nullptr;
+    char *d_c = dev_alloc_async<char>(narcs * es + 8, s);
+    short *d_mst = mst_costs_out ? dev_alloc_async<short>(narcs, s) : nullptr;
+    signed char *d_res = residues_out ? dev_alloc_async<signed char>(nres, s) : nullptr;
+    if (!d_ph || !d_corr || !d_c || (weights && !d_w) || (mst_costs_out && !d_mst) ||
+        (residues_out && !d_res))
+        rc = fail(CUPHU_ERR_ALLOC, "device allocation failed");
+    if (!rc) rc = upload_host_phase(nullptr, igram_r, igram_i, n, d_ph, gpu_id, s);
+    if (!rc) rc = copy_async(d_corr, corr, 4 * n, cudaMemcpyHostToDevice, s, "H2D corr");
+    if (!rc && weights)
+        rc = copy_async(d_w, weights, 2 * narcs, cudaMemcpyHostToDevice, s, "H2D weights");
+    if (!rc)
+        rc = launch_costs(d_ph, d_corr, d_w, nrow, ncol, cost_mode == CUPHU_COST_SMOOTH ? 0 : 1,
+                          *params, d_c, d_res, s);
+    if (!rc && d_mst)
+        rc = launch_mst_costs(reinterpret_cast<const short *>(d_c), (long long)narcs,
+                              (long)params->nshortcycle, (long)params->maxcost, d_mst, s);
+    if (!rc) rc = copy_async(costs_out, d_c, narcs * es, cudaMemcpyDeviceToHost, s, "D2H costs");
+    if (!rc && d_mst)
+        rc = copy_async(mst_costs_out, d_mst, narcs * 2, cudaMemcpyDeviceToHost, s, "D2H mst");
+    if (!rc && d_res)
+        rc = copy_async(residues_out, d_res, nres, cudaMemcpyDeviceToHost, s, "D2H residues");
+    cudaError_t e = cudaStreamSynchronize(s);
+    for (void *p : {(void *)d_ph, (void *)d_corr, (void *)d_w, (void *)d_c, (void *)d_mst,
+                    (void *)d_res})
+        if (p) cudaFreeAsync(p, s);
+    cudaStreamSynchronize(s);
+    if (!rc && e != cudaSuccess) rc = cuda_fail(e, "cuphu_mcf_inputs");
+    return rc;
+}
+
+/* ── post-passes on a stitched scene ─────────────────────────────────── */
+static int postpass_device(int which, float *unw, const unsigned char *mask, int nrow, int ncol,
+                           int ntr, int ntc, int rovl, int covl, int feather, cudaStream_t s)
+{
+    if (!unw || nrow < 1 || ncol < 1) return fail(CUPHU_ERR_INVALID, "bad arguments");
+    if (which == 1 && (ntr < 1 || ntc < 1 || rovl < 0 || covl < 0))
+        return fail(CUPHU_ERR_INVALID, "tile counts must be >= 1 and overlaps >= 0");
+    char *scratch = dev_alloc_async<char>(postpass_scratch_bytes(nrow, ncol), s);
+    if (!scratch) return fail(CUPHU_ERR_ALLOC, "device allocation failed");
+    int rc = which == 0 ? launch_fix_cycle_spikes(unw, mask, nrow, ncol, scratch, s)
+                        : launch_neighbor_feedback(unw, mask, nrow, ncol, ntr, ntc, rovl, covl,
+                                                   feather, scratch, s);
+    cudaFreeAsync(scratch, s);
+    return rc;
+}
+
+static int postpass_host(int which, float *unw, const unsigned char *mask, int nrow, int ncol,
+                         int ntr, int ntc, int rovl, int covl, int feather)
+{
+    if (!unw || nrow < 1 || ncol < 1) return fail(CUPHU_ERR_INVALID, "bad arguments");
+    int dev = 0;
+    CUPHU_TRY_CUDA(cudaGetDevice(&dev));
+    cudaStream_t s = lib_stream(dev);
+    const size_t n = (size_t)nrow * ncol;
+    float *d_u = dev_alloc_async<float>(n, s);
+    unsigned char *d_m = mask ? dev_alloc_async<unsigned char>(n, s) : nullptr;
+    int rc = (!d_u || (mask && !d_m)) ? fail(CUPHU_ERR_ALLOC, "device allocation failed") : 0;
+    if (!rc) rc = copy_async(d_u, unw, 4 * n, cudaMemcpyHostToDevice, s, "H2D unw");
+    if (!rc && mask) rc = copy_async(d_m, mask, n, cudaMemcpyHostToDevice, s, "H2D mask");
+    if (!rc) rc = postpass_device(which, d_u, d_m, nrow, ncol, ntr, ntc, rovl, covl, feather, s);
+    if (!rc) rc = copy_async(unw, d_u, 4 * n, cudaMemcpyDeviceToHost, s, "D2H unw");
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (d_u) cudaFreeAsync(d_u, s);
+    if (d_m) cudaFreeAsync(d_m, s);
+    cudaStreamSynchronize(s);
+    if (!rc && e != cudaSuccess) rc = cuda_fail(e, "post-pass");
+    return rc;
+}
+
+int cuphu_fix_cycle_spikes_device(float *d_unw, const unsigned char *d_mask, int nrow, int ncol,
+                                  void *stream)
+{
+    return postpass_device(0, d_unw, d_mask, nrow, ncol, 1, 1, 0, 0, 0, (cudaStream_t)stream);
+}
+
+int cuphu_laplace_neighbor_feedback_device(float *d_unw, const unsigned char *d_mask, int nrow,
+                                           int ncol, int ntr, int ntc, int row_ovrlp,
+                                           int col_ovrlp, int feather_px, void *stream)
+{
+    return postpass_device(1, d_unw, d_mask, nrow, ncol, ntr, ntc, row_ovrlp, col_ovrlp,
+                           feather_px, (cudaStream_t)stream);
+}
+
+int cuphu_fix_cycle_spikes_test(float *unw, const unsigned char *mask, int nrow, int ncol)
+{
+    return postpass_host(0, unw, mask, nrow, ncol, 1, 1, 0, 0, 0);
+}
+
+int cuphu_laplace_neighbor_feedback_test(float *unw, const unsigned char *mask, int nrow, int ncol,
+                                         int ntr, int ntc, int row_ovrlp, int col_ovrlp,
+                                         int feather_px)
+{
+    return postpass_host(1, unw, mask, nrow, ncol, ntr, ntc, row_ovrlp, col_ovrlp, feather_px);
 }
 
 int cuphu_phase_gpu(const float *d_igram_c64, long long n, float *d_phase, void *stream)
@@ -1216,27 +1518,25 @@ int cuphu_build_costs_gpu(const float *igram_r, const float *igram_i, const floa
     size_t n = (size_t)nrow * ncol;
     size_t narcs = (size_t)(nrow - 1) * ncol + (size_t)nrow * (ncol - 1);
     size_t es = cost_mode == CUPHU_COST_SMOOTH ? 4 : 8;
-    float *d_re = dev_alloc_async<float>(n, s), *d_im = dev_alloc_async<float>(n, s);
     float *d_corr = dev_alloc_async<float>(n, s), *d_ph = dev_alloc_async<float>(n, s);
     short *d_w = weights ? dev_alloc_async<short>(narcs, s) : nullptr;
     char *d_c = dev_alloc_async<char>(narcs * es + 8, s);
     void *h = std::malloc(narcs * es + 8);
-    if (!d_re || !d_im || !d_corr || !d_ph || !d_c || (weights && !d_w) || !h)
+    if (!d_corr || !d_ph || !d_c || (weights && !d_w) || !h)
         rc = fail(CUPHU_ERR_ALLOC, "allocation failed");
     if (!rc) {
-        rc = copy_async(d_re, igram_r, 4 * n, cudaMemcpyHostToDevice, s, "H2D igram_r");
-        if (!rc) rc = copy_async(d_im, igram_i, 4 * n, cudaMemcpyHostToDevice, s, "H2D igram_i");
+        /* the phase as the reference takes it: host atan2 (cuphu_solver.cpp:2120-2126) */
+        rc = upload_host_phase(nullptr, igram_r, igram_i, n, d_ph, gpu_id, s);
         if (!rc) rc = copy_async(d_corr, corr, 4 * n, cudaMemcpyHostToDevice, s, "H2D corr");
         if (!rc && weights)
             rc = copy_async(d_w, weights, 2 * narcs, cudaMemcpyHostToDevice, s, "H2D weights");
-        if (!rc) rc = launch_phase_split(d_re, d_im, d_ph, (long long)n, s);
     }
     if (!rc)
         rc = launch_costs(d_ph, d_corr, d_w, nrow, ncol, cost_mode == CUPHU_COST_SMOOTH ? 0 : 1,
                           *params, d_c, nullptr, s);
     if (!rc) rc = copy_async(h, d_c, narcs * es, cudaMemcpyDeviceToHost, s, "D2H costs");
     cudaError_t e = cudaStreamSynchronize(s);
-    cudaFreeAsync(d_re, s); cudaFreeAsync(d_im, s); cudaFreeAsync(d_corr, s);
+    cudaFreeAsync(d_corr, s);
     cudaFreeAsync(d_ph, s); cudaFreeAsync(d_c, s);
     if (d_w) cudaFreeAsync(d_w, s);
     if (!rc && e != cudaSuccess) rc = cuda_fail(e, "cuphu_build_costs_gpu");

@@ -147,6 +147,40 @@ __global__ void k_init_mins(int *m)
     m[1] = 32000;
 }
 
+/* Initial-flow arc weights of the network-flow front end
+ * (cuphu_solver.cpp:607-633): SNAPHU's smooth incremental costs of a +-1
+ * flow from flow 0 (the arithmetic of k_incrcost with flow 0, nflow 1, in
+ * 64-bit integers), w = clip(min(pos, neg), 1, maxcost).  Arcs with
+ * sigsq = LARGESHORT have no cost preference (pos = neg = 0) and get 1. */
+__global__ void __launch_bounds__(256) k_mst_costs(const short2 *__restrict__ costs,
+                                                   long long narcs, long long nsc,
+                                                   long long maxcost, short *out)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < narcs;
+         i += (long long)gridDim.x * blockDim.x) {
+        const short2 c = costs[i];
+        long long m = 0;
+        if (c.y != 32000) {
+            const long long off = c.x, sg = c.y;
+            const long long i1 = llabs(off), ip = llabs(nsc + off), in = llabs(off - nsc);
+            const long long c1 = (i1 * i1) / sg;
+            m = min((ip * ip) / sg - c1, (in * in) / sg - c1);
+        }
+        out[i] = (short)max(1LL, min(maxcost, m));
+    }
+}
+
+int launch_mst_costs(const short *costs, long long narcs, long nsc, long maxcost, short *out,
+                     cudaStream_t s)
+{
+    if (narcs > 0) {
+        int blocks = (int)std::min<long long>((narcs + 255) / 256, 148LL * 8);
+        k_mst_costs<<<blocks, 256, 0, s>>>(reinterpret_cast<const short2 *>(costs), narcs,
+                                           (long long)nsc, (long long)maxcost, out);
+    }
+    return cuda_fail(cudaGetLastError(), "k_mst_costs");
+}
+
 int launch_incrcost(const short *costs, const short *flows, int narcs, long nsc, int nflow,
                     short *pos, short *neg, int *scratch, cudaStream_t s)
 {

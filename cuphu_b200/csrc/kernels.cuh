@@ -40,7 +40,8 @@ struct SolverPlanes {
     float *dx;                  /* mixed: FP32 increment since the last fold */
     void *r, *p0, *p1;          /* PCG vectors, float or double; p is    */
     void *q, *diag;             /* double-buffered across iterations     */
-    void *z;                    /* z = r / diag, written by the update pass */
+    void *z;                    /* z = r / diag (mixed: first z buffer; r is the second) */
+    float *q1;                  /* mixed: second q buffer                */
     float *unw;                 /* congruent unwrapped phase per tile    */
     int32_t *cyc;               /* optional cycle map per tile           */
     float *cont;                /* optional anchored continuous solution */
@@ -50,6 +51,10 @@ struct SolverPlanes {
                                    wrapped phase differences (optional) */
     const float *rhs;           /* WLS mode: explicit right-hand side (optional) */
 };
+
+/* FP64 partial sums per solver work item: the mixed pass reduces r.z, p.q,
+ * z.q and q.(q/diag) together; every other phase uses the first component */
+constexpr int kNComp = 4;
 
 /* per-tile PCG scalars, double-buffered by iteration parity: every block
  * touching a tile derives the same values from the same partials */
@@ -61,7 +66,8 @@ struct TileState {
 struct SolverCtl {
     unsigned bar_count, bar_gen;
     int err, n_active, snap;
-    int total_iters, max_pass_iters, pad;
+    int total_iters, max_pass_iters;
+    int pass_max;                  /* largest iteration count of the current pass (mixed) */
     unsigned long long px_iters;   /* sum over tiles and passes of iterations x pixels */
 };
 
@@ -73,7 +79,12 @@ struct SolveParams {
     long long timeout_ns;       /* grid-barrier wait limit                   */
     int wls = 0;                /* raw solve: no anchor / congruence phase   */
     int warm = 0;               /* keep the caller's initial x on pass 0     */
+    int skip_block = -1;        /* failure test: this block does not arrive at
+                                   the first grid barrier (-1: none)         */
 };
+
+/* laplace.cu: arm the failure test for the next solver launch on a device */
+void solver_skip_barrier_once(int dev, int block);
 
 struct ScenePlan {
     float *unw_out;
@@ -111,6 +122,13 @@ int launch_w0(const TileDesc *tiles, const int *item_tile, int nitems, const Cos
 int launch_w0_from_costs(const short *costs, int stride, int nrow, int ncol, int pitch,
                          const SolverPlanes &P, cudaStream_t s);
 
+/* host_phase.cu: the reference's host phase of an interleaved (c64) or split
+ * (re, im) host interferogram, uploaded into d_ph on stream s */
+int upload_host_phase(const float *c64, const float *re, const float *im, size_t n, float *d_ph,
+                      int dev, cudaStream_t s);
+/* the same phase into host memory, computed by the host thread pool */
+void compute_host_phase(const float *c64, const float *re, const float *im, size_t n, float *out);
+
 /* laplace.cu */
 int launch_solve(bool fp64, const TileDesc *tiles, const int *item_tile, int nitems,
                  int ntiles, const SolverPlanes &P, int plane_pitch, int plane_rows,
@@ -138,6 +156,22 @@ int launch_merge(const ScenePlan *scenes, const ScenePlan *h_scenes, int nscenes
                  const TileDesc *tiles, const SolverPlanes &P, const double *tile_k,
                  const unsigned *comp_off, const SceneOut *sout, cudaStream_t s);
 
+/* postpass.cu: the reference's optional post-passes on a stitched scene
+ * (scene layout, device memory); scratch of postpass_scratch_bytes */
+size_t postpass_scratch_bytes(int nrow, int ncol);
+int launch_fix_cycle_spikes(float *unw, const unsigned char *mask, int nrow, int ncol,
+                            void *scratch, cudaStream_t s);
+int launch_neighbor_feedback(float *unw, const unsigned char *mask, int nrow, int ncol, int ntr,
+                             int ntc, int rovl, int covl, int feather, void *scratch,
+                             cudaStream_t s);
+/* bridge.cu: phase bridging of a stitched scene (device unw and conncomp,
+ * scene layout); synchronises the stream for its region-scale steps */
+int run_bridge(float *unw, uint32_t *cc, const unsigned char *mask, int nrow, int ncol,
+               const CuPhuBridgeParams &bp, cudaStream_t s);
+/* stitch.cu: the reference-pixel shift of a merged scene (_unwrap.py:605-617) */
+int launch_ref_shift(float *unw, const float *ph, int nrow, int ncol, int ref_row, int ref_col,
+                     SceneOut *tmp, cudaStream_t s);
+
 /* tune.cu: kind 0 = cost-kernel variant (0: 3 blocks/SM, 1: 4 blocks/SM),
  * kind 1 = persistent-solver blocks per SM; -1 = no stored choice */
 int tune_class(long long n);
@@ -157,5 +191,7 @@ int launch_integrate(const float *ph, const short *hflows, const short *vflows, 
                      int ncol, float *rowoff, float *unw, cudaStream_t s);
 int launch_incrcost(const short *costs, const short *flows, int narcs, long nsc, int nflow,
                     short *pos, short *neg, int *scratch, cudaStream_t s);
+int launch_mst_costs(const short *costs, long long narcs, long nsc, long maxcost, short *out,
+                     cudaStream_t s);
 
 }  // namespace cuphu

@@ -16,20 +16,34 @@
  *    tile reduces the item partials in fixed order) in FP64, so there are no
  *    host round trips and no float atomics (the reference does two blocking
  *    D2H syncs per iteration and accumulates dots with float atomicAdd).
- *  - The p = z + beta p update is folded into the next stencil pass: each
- *    work item rebuilds p for its halo from r, diag and the previous p in
- *    shared memory (p is double-buffered so neighbours never race).
  *  - FP64 mode keeps every vector in double and is bit-identical to the CPU
- *    FP64 oracle (same operation order, explicit fma, same reduction tree).
- *    Mixed mode stores x, r, p, q, diag in FP32 (half the bytes) with FP64
- *    scalars and dots, and replaces the recursive residual by the true
- *    residual b - A x every `replace_every` iterations.
+ *    FP64 oracle (same operation order, explicit fma, same reduction tree):
+ *    two passes and two grid barriers per iteration.  The stencil pass
+ *    rebuilds p = z + beta p_old for its item and halo in shared memory
+ *    (p is double-buffered so neighbours never race) and computes q = A p;
+ *    the update pass moves x, r and z.
+ *  - Mixed mode runs ONE pass and ONE grid barrier per iteration (a
+ *    single-synchronisation form of the same Jacobi-PCG).  The solution is an
+ *    FP64 base x plus an FP32 increment dx; z, p, q are FP32 (r = z diag is
+ *    not stored) and both z and q are double-buffered like p.  Each pass
+ *    applies the previous iteration's update (dx += alpha p_old,
+ *    z = (z diag - alpha q) / diag), folds p = z + beta p_old, own pixels and
+ *    halo alike, and computes q = A p, recomputing diag from the staged arc
+ *    weights; it reduces r.z, p.q, z.q and q.(q/diag) in FP64 in one tree.
+ *    alpha and the stop test use the true r.z of the pass; beta uses the
+ *    one-step recurrence r.z' = r.z - 2 alpha z.q + alpha^2 q.(q/diag)
+ *    anchored at that true value.  Every `replace_every` iterations the
+ *    increment is folded into x and the recursive residual is replaced by
+ *    the true residual b - A x (FP64).
  */
 #include "kernels.cuh"
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda/atomic>
+#include <atomic>
+#include <cstring>
+#include <mutex>
 #include <vector>
 
 namespace cuphu {
@@ -142,6 +156,55 @@ __device__ void seg_done(const TileDesc &T, int t, int nseg, const double *part,
     }
 }
 
+/* The kNComp block trees of one item in one barrier (the mixed pass reduces
+ * four dots per item): per component the same shuffle-down tree per warp
+ * and warp-0 tree as block_sum_item, results in thread 0.  `half` selects
+ * one of the two scratch halves, as consecutive items alternate. */
+__device__ __forceinline__ void block_sum4_item(double v[kNComp], double (*sw4)[kNComp][8],
+                                                int half)
+{
+#pragma unroll
+    for (int c = 0; c < kNComp; ++c)
+        for (int off = 16; off > 0; off >>= 1) v[c] += __shfl_down_sync(0xffffffffu, v[c], off);
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0)
+#pragma unroll
+        for (int c = 0; c < kNComp; ++c) sw4[half][c][w] = v[c];
+    __syncthreads();
+    if (w == 0) {
+#pragma unroll
+        for (int c = 0; c < kNComp; ++c) {
+            double x = lane < (int)(blockDim.x >> 5) ? sw4[half][c][lane] : 0.0;
+            for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+            v[c] = x;
+        }
+    }
+}
+
+/* seg_done for the kNComp-component partials of the mixed pass: component c
+ * of item i at part[c * nitems + i], of tile t at tot[c * ntiles + t] */
+__device__ void seg_done4(const TileDesc &T, int t, int nseg, const double *part, int nitems,
+                          double *tot, int ntiles, unsigned *cnt, double *sw, double *s_bcast,
+                          int *s_flag)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        unsigned prev = atomicAdd(&cnt[t], (unsigned)nseg);
+        int last = prev + (unsigned)nseg == (unsigned)T.nitems;
+        if (last) __threadfence();
+        *s_flag = last;
+    }
+    __syncthreads();
+    if (*s_flag) {
+        for (int c = 0; c < kNComp; ++c) {
+            double v = tile_reduce(T, part + (size_t)c * nitems, sw, s_bcast);
+            if (threadIdx.x == 0) tot[(size_t)c * ntiles + t] = v;
+        }
+        if (threadIdx.x == 0) cnt[t] = 0u;
+    }
+}
+
 __device__ __forceinline__ unsigned long long globaltimer()
 {
     unsigned long long t;
@@ -150,8 +213,12 @@ __device__ __forceinline__ unsigned long long globaltimer()
 }
 
 /* Grid barrier with a bounded wait.  The last arriving block snapshots the
- * active-tile count, so every block takes the same loop decision. */
-__device__ __forceinline__ bool grid_sync(SolverCtl *ctl, long long timeout_ns)
+ * active-tile count, so every block takes the same loop decision.  A block
+ * called with arrive = false waits without arriving (the failure test of
+ * cuphu_test_skip_barrier_once): every wait then runs out and the error
+ * status ends the kernel. */
+__device__ __forceinline__ bool grid_sync(SolverCtl *ctl, long long timeout_ns,
+                                          bool arrive = true)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -160,8 +227,8 @@ __device__ __forceinline__ bool grid_sync(SolverCtl *ctl, long long timeout_ns)
         cuda::atomic_ref<int, cuda::thread_scope_device> act(ctl->n_active);
         __threadfence();
         unsigned g = gen.load(cuda::memory_order_acquire);
-        unsigned prev = cnt.fetch_add(1u, cuda::memory_order_acq_rel);
-        if (prev == gridDim.x - 1u) {
+        unsigned prev = arrive ? cnt.fetch_add(1u, cuda::memory_order_acq_rel) : 0u;
+        if (arrive && prev == gridDim.x - 1u) {
             cnt.store(0u, cuda::memory_order_relaxed);
             *(volatile int *)&ctl->snap = act.load(cuda::memory_order_relaxed);
             gen.fetch_add(1u, cuda::memory_order_release);
@@ -201,10 +268,11 @@ __device__ __forceinline__ ItemXY item_xy(const TileDesc &T, int li)
 
 /* ── INIT / true residual: b, diag (A10) and r = b - A x, rz partial ────────
  * zero_x: first pass (x = 0, r = b).  write_diag: assemble pass (else the
- * stored diag is reused: residual replacement). */
+ * stored diag is reused: residual replacement).  z = r / diag goes to zout
+ * (mixed mode double-buffers z). */
 template <typename V, bool WLS>
 __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, bool zero_x,
-                             bool write_diag)
+                             bool write_diag, V *zout)
 {
     ItemXY q = item_xy(T, li);
     if (q.r >= T.nr || q.c0 >= T.nc) return 0.0;
@@ -293,7 +361,7 @@ __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, b
         if (write_diag) dv[j] = ds;
     }
     if (sizeof(V) == 8) st4(rr + prow + q.c0, rv);
-    st4((V *)P.z + T.pix + prow + q.c0, zv);
+    st4(zout + T.pix + prow + q.c0, zv);
     if (write_diag) st4(dg + prow + q.c0, dv);
     if (zero_x) {
         st4(x + prow + q.c0, xv);
@@ -318,59 +386,56 @@ constexpr int kSegW = kItemBx + 8;        /* stencil box width: 4 columns each s
 constexpr int kWrW = kItemBx + 4;         /* right-arc box incl. the left neighbour */
 
 struct SolveMaps {
-    CUtensorMap zA, p0A, p1A, wdA, wrA;        /* stencil pass boxes */
-    CUtensorMap xB, p0B, p1B, qB, rB, dB;      /* update pass boxes  */
-    CUtensorMap zB;                            /* mixed: z in place of r, dx in xB */
+    /* FP64 two-pass form */
+    CUtensorMap zA, p0A, p1A, wdA, wrA;        /* stencil pass boxes (zA: z buffer 0) */
+    CUtensorMap xB, p0B, p1B, qB, rB, dB;      /* update pass boxes                   */
+    /* mixed single-synchronisation pass (zA, p0A, p1A shared; xB = dx) */
+    CUtensorMap zS1, qS0, qS1;                 /* z buffer 1, q buffers 0 and 1 (halo boxes) */
+    CUtensorMap wdS, wrS;                      /* arc weights for the halo's diag as well    */
 };
 
 __host__ __device__ constexpr size_t al128(size_t b) { return (b + 127) & ~(size_t)127; }
 
-template <typename V> struct StageA {
-    static constexpr size_t kVec = al128((size_t)(kItemBy + 2) * kSegW * sizeof(V));
+/* FP64 stencil-pass stage: z and p_old with halo, down and right arc weights */
+struct StageA {
+    static constexpr size_t kVec = al128((size_t)(kItemBy + 2) * kSegW * sizeof(double));
     static constexpr size_t kWd = al128((size_t)(kItemBy + 1) * kItemBx * sizeof(float));
     static constexpr size_t kWr = al128((size_t)kItemBy * kWrW * sizeof(float));
-    /* mixed mode: the item's FP32 increment dx, which takes the previous
-     * iteration's deferred dx += alpha p_old */
-    static constexpr size_t kDx = sizeof(V) == 4 ? (size_t)kItemBy * kItemBx * 4 : 0;
-    static constexpr size_t kBytes = 2 * kVec + kWd + kWr + kDx;
-    static constexpr uint32_t kTx = (uint32_t)(2 * (kItemBy + 2) * kSegW * sizeof(V) +
+    static constexpr size_t kBytes = 2 * kVec + kWd + kWr;
+    static constexpr uint32_t kTx = (uint32_t)(2 * (kItemBy + 2) * kSegW * sizeof(double) +
                                                (kItemBy + 1) * kItemBx * 4 + kItemBy * kWrW * 4);
 };
-/* update-pass stage: FP64 mode x, p, q, r, diag; mixed mode q, z (r = z diag
- * is not stored) and diag, back to back */
-template <typename V> struct StageB {
+/* FP64 update-pass stage: x, p, q, r, diag */
+struct StageB {
     static constexpr size_t kX = (size_t)kItemBy * kItemBx * sizeof(double);
-    static constexpr size_t kV = (size_t)kItemBy * kItemBx * sizeof(V);
+    static constexpr size_t kV = (size_t)kItemBy * kItemBx * sizeof(double);
     static constexpr size_t kBytes = kX + 4 * kV;
-    static constexpr uint32_t kTxFull = (uint32_t)(sizeof(V) == 4 ? 3 * kV : kX + 4 * kV);
+    static constexpr uint32_t kTxFull = (uint32_t)(kX + 4 * kV);
     static constexpr uint32_t kTxX = (uint32_t)(kX + kV);
 };
-#ifndef CUPHU_SOLVE_STAGES_F32
-#define CUPHU_SOLVE_STAGES_F32 2
-#endif
-template <typename V> __host__ __device__ constexpr int n_stages()
-{
-    return sizeof(V) == 4 ? CUPHU_SOLVE_STAGES_F32 : 2;
-}
+/* Mixed single-synchronisation stage.  z, q, p_old and the right-arc
+ * weights as 18 x 72 boxes (rows r0b-1 .. r0b+16, columns c0b-4 .. c0b+67),
+ * the down-arc weights as a 19 x 72 box starting one row higher (the diag of
+ * a halo pixel in row r0b-1 needs the arc above it), and the item's dx. */
+struct StageS {
+    static constexpr int kBoxH = kItemBy + 2;
+    static constexpr int kWdH = kItemBy + 3;
+    static constexpr size_t kBox = al128((size_t)kBoxH * kSegW * 4);
+    static constexpr size_t kWd = al128((size_t)kWdH * kSegW * 4);
+    static constexpr size_t kDx = (size_t)kItemBy * kItemBx * 4;
+    static constexpr size_t oZ = 0, oQ = kBox, oPO = 2 * kBox, oWR = 3 * kBox, oWD = 4 * kBox;
+    static constexpr size_t oDX = 4 * kBox + kWd;
+    static constexpr size_t kBytes = al128(oDX + kDx);
+    static constexpr uint32_t kTxBox = (uint32_t)(kBoxH * kSegW * 4);
+    static constexpr uint32_t kTxWd = (uint32_t)(kWdH * kSegW * 4);
+    static constexpr uint32_t kTxDx = (uint32_t)(kItemBy * kItemBx * 4);
+};
+constexpr int kStages = 2;
 template <typename V> __host__ __device__ constexpr size_t stage_bytes()
 {
-    return al128(StageA<V>::kBytes > StageB<V>::kBytes ? StageA<V>::kBytes : StageB<V>::kBytes);
+    return sizeof(V) == 4 ? StageS::kBytes
+                          : al128(StageA::kBytes > StageB::kBytes ? StageA::kBytes : StageB::kBytes);
 }
-/* ring shape of a pass: the mixed update pass stages only q, z and diag
- * (12 KB per item), so it runs four shallow stages in the memory of the two
- * deep ones */
-constexpr size_t kStageBm = 3 * (size_t)kItemBy * kItemBx * 4;
-template <int KIND, typename V> __host__ __device__ constexpr int pass_stages()
-{
-    return (KIND == 1 && sizeof(V) == 4) ? 4 : n_stages<V>();
-}
-template <int KIND, typename V> __host__ __device__ constexpr size_t pass_stage_bytes()
-{
-    return (KIND == 1 && sizeof(V) == 4) ? kStageBm : stage_bytes<V>();
-}
-static_assert(pass_stages<1, float>() * pass_stage_bytes<1, float>() <=
-                  n_stages<float>() * stage_bytes<float>(),
-              "mixed update-pass ring exceeds the stage memory");
 /* p_new of an item with its halo ring, rows of kSegW elements laid out like
  * the staged boxes (column 0 <-> c0b - 4), so own columns start 16-byte
  * aligned at column 4 */
@@ -380,7 +445,7 @@ template <typename V> __host__ __device__ constexpr size_t pn_bytes()
 }
 template <typename V> __host__ __device__ constexpr size_t solve_smem_bytes()
 {
-    return n_stages<V>() * stage_bytes<V>() + pn_bytes<V>() + 128;
+    return kStages * stage_bytes<V>() + pn_bytes<V>() + 128;
 }
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p)
@@ -442,25 +507,22 @@ __device__ __forceinline__ void fence_async_global()
     asm volatile("fence.proxy.async.global;" ::: "memory");
 }
 
-template <typename V>
+/* ── FP64 two-pass form ───────────────────────────────────────────────── */
 __device__ __forceinline__ void issue_a(const TileDesc &T, int li, const SolveMaps &M, int pold_sel,
-                                        bool first, bool upd, char *stage, uint64_t *bar)
+                                        bool first, char *stage, uint64_t *bar)
 {
     const int r0b = (li / T.nbx) * kItemBy, c0b = (li % T.nbx) * kItemBx;
     const int y = T.row0 + r0b;
     char *Z = stage;
-    char *PO = stage + StageA<V>::kVec;
-    char *WD = PO + StageA<V>::kVec;
-    char *WR = WD + StageA<V>::kWd;
-    char *DX = WR + StageA<V>::kWr;
-    uint32_t tx = StageA<V>::kTx - (first ? (uint32_t)((kItemBy + 2) * kSegW * sizeof(V)) : 0u);
-    if (upd) tx += (uint32_t)StageA<V>::kDx;
+    char *PO = stage + StageA::kVec;
+    char *WD = PO + StageA::kVec;
+    char *WR = WD + StageA::kWd;
+    uint32_t tx = StageA::kTx - (first ? (uint32_t)((kItemBy + 2) * kSegW * sizeof(double)) : 0u);
     mbar_expect(bar, tx);
     tma_load_2d(Z, &M.zA, c0b - 4, y - 1, bar);
     if (!first) tma_load_2d(PO, pold_sel ? &M.p1A : &M.p0A, c0b - 4, y - 1, bar);
     tma_load_2d(WD, &M.wdA, c0b, y - 1, bar);
     tma_load_2d(WR, &M.wrA, c0b - 4, y, bar);
-    if (upd) tma_load_2d(DX, &M.xB, c0b, y, bar);
 }
 
 /* shared-memory vector access of 4 consecutive elements (16-byte aligned) */
@@ -476,60 +538,31 @@ __device__ __forceinline__ void sld4(const double *p, double v[4])
     v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
 
-/* p_new = z + beta p_old: FP32 arithmetic in mixed mode, FP64 in FP64 mode */
-template <typename V>
-__device__ __forceinline__ V pupdate(bool first, double beta, float betaf, V po, V z)
-{
-    if (first) return z;
-    if (sizeof(V) == 4) return (V)__fmaf_rn(betaf, (float)po, (float)z);
-    return (V)__fma_rn(beta, (double)po, (double)z);
-}
-
-/* stencil pass on a staged item: p_new = z + beta p_old (own + halo ring),
- * q = A p_new, thread partial of p.q (FP64 accumulation).  FP64 mode: FP64
- * arithmetic in the oracle's operation order.  Mixed mode: FP32 arithmetic
- * (the SpMV and vector update), FP64 only for the dot; with upd it also
- * applies the previous iteration's solution update dx += alpha_prev p_old,
- * which the update pass leaves to this pass because p_old is staged here
- * anyway. */
-template <typename V>
-__device__ double compute_a(const TileDesc &T, int li, const SolverPlanes &P, V *pnew_all,
-                            bool first, double beta, bool upd, double alpha_prev,
-                            const char *stage, V *Pn)
+/* stencil pass on a staged item (FP64, the oracle's operation order):
+ * p_new = z + beta p_old (own + halo ring), q = A p_new, thread partial of
+ * p.q */
+__device__ double compute_a(const TileDesc &T, int li, const SolverPlanes &P, double *pnew_all,
+                            bool first, double beta, const char *stage, double *Pn)
 {
     const int r0b = (li / T.nbx) * kItemBy, c0b = (li % T.nbx) * kItemBx;
-    const V *Z = (const V *)stage;
-    const V *PO = (const V *)(stage + StageA<V>::kVec);
-    const float *WD = (const float *)(stage + 2 * StageA<V>::kVec);
-    const float *WR = (const float *)(stage + 2 * StageA<V>::kVec + StageA<V>::kWd);
+    const double *Z = (const double *)stage;
+    const double *PO = (const double *)(stage + StageA::kVec);
+    const float *WD = (const float *)(stage + 2 * StageA::kVec);
+    const float *WR = (const float *)(stage + 2 * StageA::kVec + StageA::kWd);
     const int nr = T.nr, nc = T.nc;
-    const float betaf = (float)beta;
     const int ty = threadIdx.x / kItemTx, tx = threadIdx.x % kItemTx;
     const int r = r0b + ty, c0 = c0b + tx * kItemVx;
     const bool own = r < nr && c0 < nc;
     /* own p_new: row ty+1, columns 4 + 4 tx .. +3 */
-    V pn[4] = {(V)0, (V)0, (V)0, (V)0};
+    double pn[4] = {0.0, 0.0, 0.0, 0.0};
     const int so = (ty + 1) * kSegW + 4 + tx * kItemVx;
     if (own) {
-        V zv[4], pv[4] = {(V)0, (V)0, (V)0, (V)0};
+        double zv[4], pv[4] = {0.0, 0.0, 0.0, 0.0};
         sld4(Z + so, zv);
         if (!first) sld4(PO + so, pv);
 #pragma unroll
         for (int j = 0; j < kItemVx; ++j)
-            if (c0 + j < nc) pn[j] = pupdate<V>(first, beta, betaf, pv[j], zv[j]);
-        if constexpr (sizeof(V) == 4) {
-            if (upd) {
-                const float *DX = (const float *)(stage + 2 * StageA<V>::kVec + StageA<V>::kWd +
-                                                  StageA<V>::kWr);
-                float dxv[4];
-                sld4(DX + ty * kItemBx + tx * kItemVx, dxv);
-                const float af = (float)alpha_prev;
-#pragma unroll
-                for (int j = 0; j < kItemVx; ++j)
-                    if (c0 + j < nc) dxv[j] = __fmaf_rn(af, (float)pv[j], dxv[j]);
-                st4(P.dx + T.pix + (size_t)r * T.pitch + c0, dxv);
-            }
-        }
+            if (c0 + j < nc) pn[j] = first ? zv[j] : __fma_rn(beta, pv[j], zv[j]);
     }
 #pragma unroll
     for (int j = 0; j < kItemVx; ++j) Pn[so + j] = pn[j];
@@ -541,21 +574,21 @@ __device__ double compute_a(const TileDesc &T, int li, const SolverPlanes &P, V 
         else if (h < 2 * kItemBx + kItemBy) { i = 1 + h - 2 * kItemBx; jc = 3; }
         else { i = 1 + h - 2 * kItemBx - kItemBy; jc = 4 + kItemBx; }
         int gr = r0b - 1 + i, gc = c0b - 4 + jc;
-        V v = (V)0;
+        double v = 0.0;
         if (gr >= 0 && gr < nr && gc >= 0 && gc < nc) {
             int sidx = i * kSegW + jc;
-            v = pupdate<V>(first, beta, betaf, first ? (V)0 : PO[sidx], Z[sidx]);
+            v = first ? Z[sidx] : __fma_rn(beta, PO[sidx], Z[sidx]);
         }
         Pn[i * kSegW + jc] = v;
     }
     __syncthreads();
     double acc = 0.0;
     if (own) {
-        V up[4], dn[4], qv[4] = {(V)0, (V)0, (V)0, (V)0};
+        double up[4], dn[4], qv[4] = {0.0, 0.0, 0.0, 0.0};
         float wdn[4], wup[4], wrt[4];
         sld4(Pn + so - kSegW, up);
         sld4(Pn + so + kSegW, dn);
-        V lf = Pn[so - 1], rt = Pn[so + 4];
+        double lf = Pn[so - 1], rt = Pn[so + 4];
         sld4(WD + (ty + 1) * kItemBx + tx * kItemVx, wdn);
         sld4(WD + ty * kItemBx + tx * kItemVx, wup);
         sld4(WR + ty * kWrW + tx * kItemVx + 4, wrt);
@@ -564,56 +597,36 @@ __device__ double compute_a(const TileDesc &T, int li, const SolverPlanes &P, V 
         for (int j = 0; j < kItemVx; ++j) {
             int c = c0 + j;
             if (c >= nc) continue;
-            V xl = j == 0 ? lf : pn[j - 1];
-            V xr = j == kItemVx - 1 ? rt : pn[j + 1];
+            double xl = j == 0 ? lf : pn[j - 1];
+            double xr = j == kItemVx - 1 ? rt : pn[j + 1];
             float wl = j == 0 ? wlf : wrt[j - 1];
-            if (sizeof(V) == 4) {
-                float xa = (float)pn[j];
-                float y = __fmul_rn(kLapEpsF, xa);
-                if (r < nr - 1) y = __fmaf_rn(wdn[j], xa - (float)dn[j], y);
-                if (r > 0)      y = __fmaf_rn(wup[j], xa - (float)up[j], y);
-                if (c < nc - 1) y = __fmaf_rn(wrt[j], xa - (float)xr, y);
-                if (c > 0)      y = __fmaf_rn(wl, xa - (float)xl, y);
-                qv[j] = (V)y;
-            } else {
-                double xa = (double)pn[j];
-                double y = (double)kLapEpsF * xa;
-                if (r < nr - 1) y = __fma_rn((double)wdn[j], xa - (double)dn[j], y);
-                if (r > 0)      y = __fma_rn((double)wup[j], xa - (double)up[j], y);
-                if (c < nc - 1) y = __fma_rn((double)wrt[j], xa - (double)xr, y);
-                if (c > 0)      y = __fma_rn((double)wl, xa - (double)xl, y);
-                qv[j] = (V)y;
-            }
-            acc = __fma_rn((double)pn[j], (double)qv[j], acc);
+            double xa = pn[j];
+            double y = (double)kLapEpsF * xa;
+            if (r < nr - 1) y = __fma_rn((double)wdn[j], xa - dn[j], y);
+            if (r > 0)      y = __fma_rn((double)wup[j], xa - up[j], y);
+            if (c < nc - 1) y = __fma_rn((double)wrt[j], xa - xr, y);
+            if (c > 0)      y = __fma_rn((double)wl, xa - xl, y);
+            qv[j] = y;
+            acc = __fma_rn(pn[j], y, acc);
         }
         size_t o = T.pix + (size_t)r * T.pitch + c0;
         st4(pnew_all + o, pn);
-        st4((V *)P.q + o, qv);
+        st4((double *)P.q + o, qv);
     }
     return acc;
 }
 
-template <typename V>
 __device__ __forceinline__ void issue_b(const TileDesc &T, int li, const SolveMaps &M, int pnew_sel,
                                         bool update_r, char *stage, uint64_t *bar)
 {
     const int r0b = (li / T.nbx) * kItemBy, c0b = (li % T.nbx) * kItemBx;
     const int y = T.row0 + r0b;
-    if (sizeof(V) == 4) {
-        /* mixed: q, z, diag back to back */
-        char *QB = stage;
-        mbar_expect(bar, StageB<V>::kTxFull);
-        tma_load_2d(QB, &M.qB, c0b, y, bar);
-        tma_load_2d(QB + StageB<V>::kV, &M.zB, c0b, y, bar);
-        tma_load_2d(QB + 2 * StageB<V>::kV, &M.dB, c0b, y, bar);
-        return;
-    }
     char *X = stage;
-    char *PB = X + StageB<V>::kX;
-    char *QB = PB + StageB<V>::kV;
-    char *RB = QB + StageB<V>::kV;
-    char *DB = RB + StageB<V>::kV;
-    mbar_expect(bar, update_r ? StageB<V>::kTxFull : StageB<V>::kTxX);
+    char *PB = X + StageB::kX;
+    char *QB = PB + StageB::kV;
+    char *RB = QB + StageB::kV;
+    char *DB = RB + StageB::kV;
+    mbar_expect(bar, update_r ? StageB::kTxFull : StageB::kTxX);
     tma_load_2d(X, &M.xB, c0b, y, bar);
     tma_load_2d(PB, pnew_sel ? &M.p1B : &M.p0B, c0b, y, bar);
     if (update_r) {
@@ -623,69 +636,210 @@ __device__ __forceinline__ void issue_b(const TileDesc &T, int li, const SolveMa
     }
 }
 
-template <typename V>
+/* update pass (FP64): x += alpha p; r -= alpha q; z = r / diag; partial r.z */
 __device__ double compute_b(const TileDesc &T, int li, const SolverPlanes &P, double alpha,
                             bool update_r, const char *stage)
 {
     const int r0b = (li / T.nbx) * kItemBy, c0b = (li % T.nbx) * kItemBx;
-    const V *PB = (const V *)(stage + StageB<V>::kX);
-    const V *QB = PB + kItemBy * kItemBx;
-    const V *RB = QB + kItemBy * kItemBx;
-    const V *DB = RB + kItemBy * kItemBx;
+    const double *X = (const double *)stage;
+    const double *PB = (const double *)(stage + StageB::kX);
+    const double *QB = PB + kItemBy * kItemBx;
+    const double *RB = QB + kItemBy * kItemBx;
+    const double *DB = RB + kItemBy * kItemBx;
     const int ty = threadIdx.x / kItemTx, tx = threadIdx.x % kItemTx;
     const int r = r0b + ty, c0 = c0b + tx * kItemVx;
     if (r >= T.nr || c0 >= T.nc) return 0.0;
     const int s0 = ty * kItemBx + tx * kItemVx;
     const size_t o = T.pix + (size_t)r * T.pitch + c0;
     double acc = 0.0;
-    if constexpr (sizeof(V) == 4) {
-        /* mixed: r = z diag, r -= alpha q, z = r / diag (the solution update
-         * dx += alpha p is deferred to the next stencil pass or fold) */
-        const float *QM = (const float *)stage;
-        float qv[4], zv[4], dv[4];
-        sld4(QM + s0, qv);
-        sld4(QM + kItemBy * kItemBx + s0, zv);
-        sld4(QM + 2 * kItemBy * kItemBx + s0, dv);
-        const float alphaf = (float)alpha;
+    double xv[4], pv[4], qv[4], rv[4] = {0.0, 0.0, 0.0, 0.0}, dv[4], zv[4] = {0.0, 0.0, 0.0, 0.0};
+    sld4(X + s0, xv);
+    sld4(PB + s0, pv);
+    if (update_r) {
+        sld4(QB + s0, qv);
+        sld4(RB + s0, rv);
+        sld4(DB + s0, dv);
+    }
 #pragma unroll
-        for (int j = 0; j < kItemVx; ++j) {
-            if (c0 + j >= T.nc) continue;
-            float rn = __fmaf_rn(-alphaf, qv[j], __fmul_rn(zv[j], dv[j]));
-            float z = __fdiv_rn(rn, dv[j]);
+    for (int j = 0; j < kItemVx; ++j) {
+        if (c0 + j >= T.nc) continue;
+        xv[j] = __fma_rn(alpha, pv[j], xv[j]);
+        if (update_r) {
+            double rn = __fma_rn(-alpha, qv[j], rv[j]);
+            rv[j] = rn;
+            double z = rn / dv[j];
             zv[j] = z;
-            acc = __fma_rn((double)rn, (double)z, acc);
-        }
-        st4((float *)P.z + o, zv);
-    } else {
-        const double *X = (const double *)stage;
-        double xv[4];
-        V pv[4], qv[4], rv[4] = {(V)0, (V)0, (V)0, (V)0}, dv[4], zv[4] = {(V)0, (V)0, (V)0, (V)0};
-        sld4(X + s0, xv);
-        sld4(PB + s0, pv);
-        if (update_r) {
-            sld4(QB + s0, qv);
-            sld4(RB + s0, rv);
-            sld4(DB + s0, dv);
-        }
-#pragma unroll
-        for (int j = 0; j < kItemVx; ++j) {
-            if (c0 + j >= T.nc) continue;
-            xv[j] = __fma_rn(alpha, (double)pv[j], xv[j]);
-            if (update_r) {
-                V rn = (V)__fma_rn(-alpha, (double)qv[j], (double)rv[j]);
-                rv[j] = rn;
-                double z = (double)rn / (double)dv[j];
-                zv[j] = (V)z;
-                acc = __fma_rn((double)rn, z, acc);
-            }
-        }
-        st4(P.x + o, xv);
-        if (update_r) {
-            st4((V *)P.r + o, rv);
-            st4((V *)P.z + o, zv);
+            acc = __fma_rn(rn, z, acc);
         }
     }
+    st4(P.x + o, xv);
+    if (update_r) {
+        st4((double *)P.r + o, rv);
+        st4((double *)P.z + o, zv);
+    }
     return acc;
+}
+
+/* ── mixed single-synchronisation pass ─────────────────────────────────────
+ * zsel: z buffer to read (the pass writes the other); ksel: p_old and q_old
+ * buffer (p and q of the previous pass; the pass writes the other); first:
+ * no p_old (first pass of a solve); fresh: z comes straight from a residual
+ * (solve start or replacement), so there is no update to apply and no
+ * q_old or dx to stage. */
+__device__ __forceinline__ void issue_s(const TileDesc &T, int li, const SolveMaps &M, int zsel,
+                                        int ksel, bool first, bool fresh, char *stage,
+                                        uint64_t *bar)
+{
+    const int r0b = (li / T.nbx) * kItemBy, c0b = (li % T.nbx) * kItemBx;
+    const int y = T.row0 + r0b;
+    uint32_t tx = 2 * StageS::kTxBox + StageS::kTxWd;
+    if (!first) tx += StageS::kTxBox;
+    if (!fresh) tx += StageS::kTxBox + StageS::kTxDx;
+    mbar_expect(bar, tx);
+    tma_load_2d(stage + StageS::oZ, zsel ? &M.zS1 : &M.zA, c0b - 4, y - 1, bar);
+    if (!fresh) tma_load_2d(stage + StageS::oQ, ksel ? &M.qS1 : &M.qS0, c0b - 4, y - 1, bar);
+    if (!first) tma_load_2d(stage + StageS::oPO, ksel ? &M.p1A : &M.p0A, c0b - 4, y - 1, bar);
+    tma_load_2d(stage + StageS::oWR, &M.wrS, c0b - 4, y - 1, bar);
+    tma_load_2d(stage + StageS::oWD, &M.wdS, c0b - 4, y - 2, bar);
+    if (!fresh) tma_load_2d(stage + StageS::oDX, &M.xB, c0b, y, bar);
+}
+
+/* Jacobi diagonal of pixel (r, c) from its four arc weights, in the
+ * assembly's order and arithmetic (phase_init): an FP64 sum of the positive
+ * weights of the arcs inside the tile, plus eps, rounded to float */
+__device__ __forceinline__ float diag_of(int r, int c, int nr, int nc, float wdn, float wup,
+                                         float wrt, float wlf)
+{
+    double ws = 0.0;
+    if (r < nr - 1 && wdn > 0.0f) ws += wdn;
+    if (r > 0 && wup > 0.0f) ws += wup;
+    if (c < nc - 1 && wrt > 0.0f) ws += wrt;
+    if (c > 0 && wlf > 0.0f) ws += wlf;
+    return (float)(ws + (double)kLapEpsF);
+}
+
+/* One item of the mixed pass.  FP32 arithmetic for the vector updates and
+ * the stencil (IEEE round-to-nearest per operation), FP64 accumulation of
+ * the four dots: acc[0] r.z of the updated residual (when not fresh),
+ * acc[1] p.q, acc[2] z.q, acc[3] q.(q/diag). */
+__device__ __forceinline__ void compute_s(const TileDesc &T, int li, float *pnew_all,
+                                          float *znew_all, float *qnew_all, float *dx_all,
+                                          bool first, bool fresh, float alphaf, float betaf,
+                                          const char *stage, float *Pn, double acc[kNComp])
+{
+    const int r0b = (li / T.nbx) * kItemBy, c0b = (li % T.nbx) * kItemBx;
+    const float *Z = (const float *)(stage + StageS::oZ);
+    const float *Q = (const float *)(stage + StageS::oQ);
+    const float *PO = (const float *)(stage + StageS::oPO);
+    const float *WR = (const float *)(stage + StageS::oWR);
+    const float *WD = (const float *)(stage + StageS::oWD);
+    const float *DX = (const float *)(stage + StageS::oDX);
+    const int nr = T.nr, nc = T.nc;
+    const int ty = threadIdx.x / kItemTx, tx = threadIdx.x % kItemTx;
+    const int r = r0b + ty, c0 = c0b + tx * kItemVx;
+    const bool own = r < nr && c0 < nc;
+    /* halo-box coordinates: row i <-> pixel row r0b - 1 + i (the down-arc
+     * box starts one row higher: its row i + 1 holds row r0b - 1 + i),
+     * column jc <-> c0b - 4 + jc */
+    const int so = (ty + 1) * kSegW + 4 + tx * kItemVx;
+    const int sd = so + kSegW;                 /* wd(r, c) in the down-arc box */
+    /* only z' and diag of the own pixels stay in registers across the
+     * barrier; p' and the weights are read back from shared memory */
+    float zn[4] = {0.f, 0.f, 0.f, 0.f}, dg[4] = {1.f, 1.f, 1.f, 1.f};
+    const size_t o = T.pix + (size_t)r * T.pitch + c0;
+    {
+        float pn[4] = {0.f, 0.f, 0.f, 0.f};
+        if (own) {
+            float wdn[4], wup[4], wrt[4];
+            sld4(WD + sd, wdn);
+            sld4(WD + sd - kSegW, wup);
+            sld4(WR + so, wrt);
+            const float wlf = WR[so - 1];
+            float zv[4], qv[4] = {0.f, 0.f, 0.f, 0.f}, pv[4] = {0.f, 0.f, 0.f, 0.f};
+            float dxv[4] = {0.f, 0.f, 0.f, 0.f};
+            sld4(Z + so, zv);
+            if (!fresh) {
+                sld4(Q + so, qv);
+                sld4(DX + ty * kItemBx + tx * kItemVx, dxv);
+            }
+            if (!first) sld4(PO + so, pv);
+#pragma unroll
+            for (int j = 0; j < kItemVx; ++j) {
+                const int c = c0 + j;
+                if (c >= nc) continue;
+                const float d = diag_of(r, c, nr, nc, wdn[j], wup[j], wrt[j], j == 0 ? wlf : wrt[j - 1]);
+                float z = zv[j];
+                if (!fresh) {
+                    const float rn = __fmaf_rn(-alphaf, qv[j], __fmul_rn(z, d));
+                    z = __fdiv_rn(rn, d);
+                    acc[0] = __fma_rn((double)rn, (double)z, acc[0]);
+                    dxv[j] = __fmaf_rn(alphaf, pv[j], dxv[j]);
+                }
+                zn[j] = z;
+                dg[j] = d;
+                pn[j] = first ? z : __fmaf_rn(betaf, pv[j], z);
+            }
+            if (!fresh) {
+                st4(dx_all + o, dxv);
+                st4(znew_all + o, zn);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kItemVx; ++j) Pn[so + j] = pn[j];
+    }
+    /* halo ring: the same update and fold, so neighbours agree bit for bit */
+    if (threadIdx.x < 2 * kItemBx + 2 * kItemBy) {
+        int h = threadIdx.x, i, jc;
+        if (h < kItemBx) { i = 0; jc = 4 + h; }
+        else if (h < 2 * kItemBx) { i = kItemBy + 1; jc = 4 + h - kItemBx; }
+        else if (h < 2 * kItemBx + kItemBy) { i = 1 + h - 2 * kItemBx; jc = 3; }
+        else { i = 1 + h - 2 * kItemBx - kItemBy; jc = 4 + kItemBx; }
+        const int gr = r0b - 1 + i, gc = c0b - 4 + jc;
+        float v = 0.f;
+        if (gr >= 0 && gr < nr && gc >= 0 && gc < nc) {
+            const int sidx = i * kSegW + jc;
+            float z = Z[sidx];
+            if (!fresh) {
+                const float d = diag_of(gr, gc, nr, nc, WD[sidx + kSegW], WD[sidx], WR[sidx],
+                                        WR[sidx - 1]);
+                z = __fdiv_rn(__fmaf_rn(-alphaf, Q[sidx], __fmul_rn(z, d)), d);
+            }
+            v = first ? z : __fmaf_rn(betaf, PO[sidx], z);
+        }
+        Pn[i * kSegW + jc] = v;
+    }
+    __syncthreads();
+    if (own) {
+        float pn[4], up[4], dn[4], wdn[4], wup[4], wrt[4], qv[4] = {0.f, 0.f, 0.f, 0.f};
+        sld4(Pn + so, pn);
+        sld4(Pn + so - kSegW, up);
+        sld4(Pn + so + kSegW, dn);
+        const float lf = Pn[so - 1], rt = Pn[so + 4];
+        sld4(WD + sd, wdn);
+        sld4(WD + sd - kSegW, wup);
+        sld4(WR + so, wrt);
+        const float wlf = WR[so - 1];
+#pragma unroll
+        for (int j = 0; j < kItemVx; ++j) {
+            const int c = c0 + j;
+            if (c >= nc) continue;
+            const float xl = j == 0 ? lf : pn[j - 1];
+            const float xr = j == kItemVx - 1 ? rt : pn[j + 1];
+            const float wl = j == 0 ? wlf : wrt[j - 1];
+            const float xa = pn[j];
+            float y = __fmul_rn(kLapEpsF, xa);
+            if (r < nr - 1) y = __fmaf_rn(wdn[j], __fsub_rn(xa, dn[j]), y);
+            if (r > 0)      y = __fmaf_rn(wup[j], __fsub_rn(xa, up[j]), y);
+            if (c < nc - 1) y = __fmaf_rn(wrt[j], __fsub_rn(xa, xr), y);
+            if (c > 0)      y = __fmaf_rn(wl, __fsub_rn(xa, xl), y);
+            qv[j] = y;
+            acc[1] = __fma_rn((double)xa, (double)y, acc[1]);
+            acc[2] = __fma_rn((double)zn[j], (double)y, acc[2]);
+            acc[3] = __fma_rn((double)y, (double)__fdiv_rn(y, dg[j]), acc[3]);
+        }
+        st4(pnew_all + o, pn);
+        st4(qnew_all + o, qv);
+    }
 }
 
 /* mixed precision: fold the FP32 increment into the FP64 solution, optionally
@@ -948,27 +1102,20 @@ __device__ __forceinline__ Cursor cursor_active(Cursor c, const SliceCtl &sc, co
     return c;
 }
 
-/* mixed mode: the stencil pass of an iteration applies the previous
- * iteration's deferred solution update unless there is none (first
- * iteration, or alpha_prev zeroed because a fold already applied it) */
-template <typename V> __device__ __forceinline__ bool defer_upd(bool first, double alpha_prev)
-{
-    return sizeof(V) == 4 && !first && alpha_prev != 0.0;
-}
-
-/* run a staged pass over this block's slice.  KIND 0: the stencil pass,
- * KIND 1: the update pass.  NS items are in flight; the stage of item k is
- * refilled with item k+NS right after the barrier of item k's reduction,
- * which every thread reaches only after its last read of the stage and Pn. */
-template <int KIND, typename V>
+/* run a staged FP64 pass over this block's slice.  KIND 0: the stencil
+ * pass, KIND 1: the update pass.  kStages items are in flight; the stage of
+ * item k is refilled with item k+kStages right after the barrier of item k's
+ * reduction, which every thread reaches only after its last read of the
+ * stage and Pn. */
+template <int KIND>
 __device__ void run_pass(const SliceCtl &sc, const TileDesc *gt, const TileState *st, int ntiles,
-                         const SolverPlanes &P, const SolveMaps &M, int psel, V *pvec, bool flag,
-                         double *part, double *tot, unsigned *cnt, double *sw, double *s_bcast,
-                         int *s_flag, V *Pn, char *stages, uint64_t *bars, uint32_t &parity,
-                         SolverCtl *ctl, long long timeout_ns)
+                         const SolverPlanes &P, const SolveMaps &M, int psel, double *pvec,
+                         bool flag, double *part, double *tot, unsigned *cnt, double *sw,
+                         double *s_bcast, int *s_flag, double *Pn, char *stages, uint64_t *bars,
+                         uint32_t &parity, SolverCtl *ctl, long long timeout_ns)
 {
-    constexpr int NS = pass_stages<KIND, V>();
-    constexpr size_t SB = pass_stage_bytes<KIND, V>();
+    constexpr int NS = kStages;
+    constexpr size_t SB = stage_bytes<double>();
     const bool red = KIND == 0 || flag;
     if (sc.s0 >= sc.s1) return;
     Cursor ci = cursor_active(Cursor{sc.s0, sc.t0}, sc, gt, st, ntiles);
@@ -982,10 +1129,8 @@ __device__ void run_pass(const SliceCtl &sc, const TileDesc *gt, const TileState
         if (threadIdx.x == 0) {
             const TileDesc &T = stile(sc, gt, ci.t);
             int li = ci.p - sc.pre[ci.t];
-            if (KIND == 0)
-                issue_a<V>(T, li, M, psel, flag, defer_upd<V>(flag, salpha(sc, st, ci.t)),
-                           stages + k * SB, bars + k);
-            else issue_b<V>(T, li, M, psel, flag, stages + k * SB, bars + k);
+            if (KIND == 0) issue_a(T, li, M, psel, flag, stages + k * SB, bars + k);
+            else issue_b(T, li, M, psel, flag, stages + k * SB, bars + k);
         }
         ci = cursor_active(Cursor{ci.p + 1, ci.t}, sc, gt, st, ntiles);
     }
@@ -998,12 +1143,10 @@ __device__ void run_pass(const SliceCtl &sc, const TileDesc *gt, const TileState
         const TileDesc &T = stile(sc, gt, cc.t);
         int li = cc.p - sc.pre[cc.t];
         double acc;
-        if (KIND == 0) {
-            const double ap = salpha(sc, st, cc.t);
-            acc = compute_a<V>(T, li, P, pvec, flag, sbeta(sc, st, cc.t), defer_upd<V>(flag, ap),
-                               ap, stages + s * SB, Pn);
-        } else
-            acc = compute_b<V>(T, li, P, salpha(sc, st, cc.t), flag, stages + s * SB);
+        if (KIND == 0)
+            acc = compute_a(T, li, P, pvec, flag, sbeta(sc, st, cc.t), stages + s * SB, Pn);
+        else
+            acc = compute_b(T, li, P, salpha(sc, st, cc.t), flag, stages + s * SB);
         double bs = block_sum_item(acc, sw + 8 * (done & 1));   /* contains the item barrier */
         if (threadIdx.x == 0) {
             if (red) part[T.item0 + li] = bs;
@@ -1011,10 +1154,8 @@ __device__ void run_pass(const SliceCtl &sc, const TileDesc *gt, const TileState
                 fence_async_smem();
                 const TileDesc &Tn = stile(sc, gt, ci.t);
                 int ln = ci.p - sc.pre[ci.t];
-                if (KIND == 0)
-                    issue_a<V>(Tn, ln, M, psel, flag, defer_upd<V>(flag, salpha(sc, st, ci.t)),
-                               stages + s * SB, bars + s);
-                else issue_b<V>(Tn, ln, M, psel, flag, stages + s * SB, bars + s);
+                if (KIND == 0) issue_a(Tn, ln, M, psel, flag, stages + s * SB, bars + s);
+                else issue_b(Tn, ln, M, psel, flag, stages + s * SB, bars + s);
             }
         }
         if (ci.p < sc.s1) ci = cursor_active(Cursor{ci.p + 1, ci.t}, sc, gt, st, ntiles);
@@ -1029,70 +1170,63 @@ __device__ void run_pass(const SliceCtl &sc, const TileDesc *gt, const TileState
     __syncthreads();
 }
 
-/* Mixed-precision update pass without shared-memory staging.  The pass is
- * elementwise (r = z diag - alpha q, z = r / diag) plus the r.z dot, so the
- * block sweeps its slice's pixel rows with 16-byte loads straight from HBM
- * (contiguous row spans per plane instead of 256-byte item rows), and
- * each thread accumulates r.z in FP64 over the whole tile segment: one block reduction
- * per tile segment instead of one per item, no barrier per item.  The
- * segment total goes into the partial slot of the segment's first item and
- * the segment's other slots are zeroed, so the tile total is the canonical
- * sum over the tile's partials as in the other phases (deterministic for a
- * given grid; mixed mode does not follow the oracle's summation order). */
-__device__ void run_update_direct(const SliceCtl &sc, const TileDesc *gt, const TileState *st,
-                                  const SolverPlanes &P, double *part, double *tot,
-                                  unsigned *cnt, double *sw, double *s_bcast, int *s_flag)
+/* the mixed single-synchronisation pass over this block's slice, staged
+ * like run_pass, with kNComp partials per item */
+__device__ void run_pass_s(const SliceCtl &sc, const TileDesc *gt, const TileState *st, int ntiles,
+                           int nitems, const SolveMaps &M, int zsel, int ksel, bool first,
+                           bool fresh, float *pnew, float *znew, float *qnew, float *dx,
+                           double *part, double *tot, unsigned *cnt, double *sw,
+                           double (*sw4)[kNComp][8], double *s_bcast, int *s_flag, float *Pn,
+                           char *stages, uint64_t *bars, uint32_t &parity, SolverCtl *ctl,
+                           long long timeout_ns)
 {
-    for (int t = sc.t0; t <= sc.t1; ++t) {
-        if (sc.pre[t + 1] == sc.pre[t] || !sactive(sc, st, t)) continue;
-        const TileDesc &T = stile(sc, gt, t);
-        int a, b;
-        slice_items(sc, T, t, a, b);
-        if (a >= b) continue;
-        const float alphaf = (float)salpha(sc, st, t);
-        const int nr = T.nr, nc = T.nc, nbx = T.nbx;
-        float *zp = (float *)P.z + T.pix;
-        const float *qp = (const float *)P.q + T.pix, *dp = (const float *)P.diag + T.pix;
-        double acc = 0.0;
-        /* the segment's items, band by band (16-row strips), each strip swept
-         * one pixel row at a time across the segment's columns of the band */
-        for (int band = a / nbx; band <= (b - 1) / nbx; ++band) {
-            const int i0 = max(a, band * nbx) - band * nbx, i1 = min(b, (band + 1) * nbx) - band * nbx;
-            const int clo = i0 * kItemBx, chi = min(i1 * kItemBx, nc);
-            const int rlo = band * kItemBy, rhi = min(rlo + kItemBy, nr);
-            /* the band's (row, 4-column group) pairs spread over all threads,
-             * row-major, so partial bands keep every thread busy */
-            const int qw = (chi - clo + kItemVx - 1) / kItemVx;
-            const int nq = (rhi - rlo) * qw;
-            for (int u = threadIdx.x; u < nq; u += blockDim.x) {
-                {
-                    const int r = rlo + u / qw, c0 = clo + (u - (u / qw) * qw) * kItemVx;
-                    const size_t o = (size_t)r * T.pitch + c0;
-                    float4 qv = __ldcs(reinterpret_cast<const float4 *>(qp + o));
-                    float4 zv = __ldcg(reinterpret_cast<const float4 *>(zp + o));
-                    float4 dv = __ldcg(reinterpret_cast<const float4 *>(dp + o));
-                    const int n4 = min(chi - c0, kItemVx);
-                    float q4[4] = {qv.x, qv.y, qv.z, qv.w};
-                    float z4[4] = {zv.x, zv.y, zv.z, zv.w};
-                    float d4[4] = {dv.x, dv.y, dv.z, dv.w};
+    constexpr int NS = kStages;
+    constexpr size_t SB = stage_bytes<float>();
+    if (sc.s0 >= sc.s1) return;
+    Cursor ci = cursor_active(Cursor{sc.s0, sc.t0}, sc, gt, st, ntiles);
+    if (ci.p >= sc.s1) return;
+    Cursor cc = ci;
+    if (threadIdx.x == 0) {
+        fence_async_global();
+        fence_async_smem();
+    }
+    for (int k = 0; k < NS && ci.p < sc.s1; ++k) {
+        if (threadIdx.x == 0)
+            issue_s(stile(sc, gt, ci.t), ci.p - sc.pre[ci.t], M, zsel, ksel, first, fresh,
+                    stages + k * SB, bars + k);
+        ci = cursor_active(Cursor{ci.p + 1, ci.t}, sc, gt, st, ntiles);
+    }
+    int done = 0;
+    while (cc.p < sc.s1) {
+        int s = done % NS;
+        mbar_wait(bars + s, (parity >> s) & 1u, ctl, timeout_ns);
+        parity ^= 1u << s;
+        ++done;
+        const TileDesc &T = stile(sc, gt, cc.t);
+        int li = cc.p - sc.pre[cc.t];
+        double acc[kNComp] = {0.0, 0.0, 0.0, 0.0};
+        compute_s(T, li, pnew, znew, qnew, dx, first, fresh, (float)salpha(sc, st, cc.t),
+                  (float)sbeta(sc, st, cc.t), stages + s * SB, Pn, acc);
+        block_sum4_item(acc, sw4, done & 1);   /* contains the item barrier */
+        if (threadIdx.x == 0) {
 #pragma unroll
-                    for (int j = 0; j < kItemVx; ++j) {
-                        if (j >= n4) continue;
-                        float rn = __fmaf_rn(-alphaf, q4[j], __fmul_rn(z4[j], d4[j]));
-                        float z = __fdiv_rn(rn, d4[j]);
-                        z4[j] = z;
-                        acc = __fma_rn((double)rn, (double)z, acc);
-                    }
-                    st4(zp + o, z4);
-                }
+            for (int c = 0; c < kNComp; ++c) part[(size_t)c * nitems + T.item0 + li] = acc[c];
+            if (ci.p < sc.s1) {
+                fence_async_smem();
+                issue_s(stile(sc, gt, ci.t), ci.p - sc.pre[ci.t], M, zsel, ksel, first, fresh,
+                        stages + s * SB, bars + s);
             }
         }
-        double v = block_sum(acc, sw);
-        if (threadIdx.x == 0) part[T.item0 + a] = v;
-        for (int li = a + 1 + (int)threadIdx.x; li < b; li += blockDim.x) part[T.item0 + li] = 0.0;
-        __threadfence();
-        seg_done(T, t, b - a, part, tot, cnt, sw, s_bcast, s_flag);
+        if (ci.p < sc.s1) ci = cursor_active(Cursor{ci.p + 1, ci.t}, sc, gt, st, ntiles);
+        Cursor nx = cursor_active(Cursor{cc.p + 1, cc.t}, sc, gt, st, ntiles);
+        if (nx.p >= sc.s1 || nx.t != cc.t) {
+            int a, b;
+            slice_items(sc, T, cc.t, a, b);
+            seg_done4(T, cc.t, b - a, part, nitems, tot, ntiles, cnt, sw, s_bcast, s_flag);
+        }
+        cc = nx;
     }
+    __syncthreads();
 }
 
 /* state written by other blocks before the last grid barrier: read from L2 */
@@ -1113,6 +1247,54 @@ __device__ __forceinline__ TileState load_state(const TileState *p)
 #define CUPHU_SOLVE_MIN_BLOCKS 3
 #endif
 
+/* A tile leaves the solve: the owner block updates the active count and the
+ * statistics (pixel-iterations, the pass's largest iteration count). */
+__device__ __forceinline__ void tile_stop(TileState &S, const TileDesc &T, bool owner,
+                                          SolverCtl *ctl)
+{
+    S.active = 0;
+    if (owner && threadIdx.x == 0) {
+        atomicSub(&ctl->n_active, 1);
+        atomicAdd(&ctl->px_iters,
+                  (unsigned long long)S.iter * (unsigned long long)((long long)T.nr * T.nc));
+        atomicMax(&ctl->pass_max, S.iter);
+    }
+}
+
+/* first scalars of a solve from the tile's initial r.z */
+__device__ __forceinline__ TileState start_state(double rz, const SolveParams &sp)
+{
+    TileState S;
+    S.rz = rz;
+    S.rz0 = rz;
+    S.thr = (double)sp.tol * (double)sp.tol * rz;
+    S.alpha = 0.0;
+    S.beta = 0.0;
+    S.iter = 0;
+    S.active = (rz > 0.0 && sp.max_iter > 0) ? 1 : 0;
+    return S;
+}
+
+/* publish a tile's new scalars: the owner (or a block beyond its cache)
+ * stores them; every block touching the tile caches its own copy */
+__device__ __forceinline__ void put_state(SliceCtl &sc, TileState *dst, int t, const TileState &S,
+                                          bool owner)
+{
+    if (threadIdx.x == 0) {
+        if (owner || !scached(sc, t)) dst[t] = S;
+        sput(sc, t, S);
+    }
+}
+
+/* tiles not counted by a phase that slices over the active tiles of `from`
+ * keep their inactive flag in `to` */
+__device__ __forceinline__ void carry_inactive(const TileState *from, TileState *to, int ntiles)
+{
+    if (blockIdx.x == 0)
+        for (int t = threadIdx.x; t < ntiles; t += blockDim.x)
+            if (!__ldcg(&from[t].active)) to[t].active = 0;
+}
+
 /* WLS = true: the WLS-mode instance (explicit arc targets / right-hand
  * side, optional warm start, no anchoring); a separate instantiation so the
  * main path's register allocation does not carry its extra inputs */
@@ -1124,25 +1306,30 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
 {
     extern __shared__ __align__(128) char dsm_raw[];
     __shared__ double sw[32];
+    __shared__ double sw4[2][kNComp][8];
     __shared__ double s_bcast;
     __shared__ int s_flag;
-    __shared__ __align__(8) uint64_t bars[4];
+    __shared__ __align__(8) uint64_t bars[kStages];
     __shared__ SliceCtl sc;
-    constexpr int NS = n_stages<V>();
-    constexpr int NBAR = pass_stages<1, V>() > NS ? pass_stages<1, V>() : NS;
     char *dsm = (char *)(((uintptr_t)dsm_raw + 127) & ~(uintptr_t)127);
-    const bool mixed = sizeof(V) == 4;
+    constexpr bool mixed = sizeof(V) == 4;
     V *pb[2] = {(V *)P.p0, (V *)P.p1};
-    /* per-item partials and published tile totals, both double-buffered by
-     * phase parity, and the per-tile item tickets */
-    double *pbuf[2] = {part, part + nitems};
-    double *tbuf[2] = {part + 2 * (size_t)nitems, part + 2 * (size_t)nitems + ntiles};
-    unsigned *tick = reinterpret_cast<unsigned *>(part + 2 * (size_t)nitems + 2 * (size_t)ntiles);
-    V *Pn = (V *)(dsm + NS * stage_bytes<V>());
+    /* per-item partials (kNComp components, component-major) and published
+     * tile totals, both double-buffered by phase parity, and the per-tile
+     * item tickets */
+    double *pbuf[2] = {part, part + (size_t)kNComp * nitems};
+    double *tbuf[2] = {part + 2 * (size_t)kNComp * nitems,
+                       part + 2 * (size_t)kNComp * nitems + (size_t)kNComp * ntiles};
+    unsigned *tick = reinterpret_cast<unsigned *>(part + 2 * (size_t)kNComp * nitems +
+                                                  2 * (size_t)kNComp * ntiles);
+    V *Pn = (V *)(dsm + kStages * stage_bytes<V>());
+    /* z buffers: the first is written by the assembly; mixed mode
+     * double-buffers z in the r plane (r = z diag is not stored) */
+    V *zb[2] = {(V *)P.z, (V *)P.r};
     uint32_t parity = 0u;
     (void)item_tile;
     if (threadIdx.x == 0) {
-        for (int k = 0; k < NBAR; ++k) mbar_init(&bars[k]);
+        for (int k = 0; k < kStages; ++k) mbar_init(&bars[k]);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -1156,168 +1343,217 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
             int a, b;
             slice_items(sc, T, t, a, b);
             for (int li = a; li < b; ++li)
-                store_partial(phase_init<V, WLS>(T, li, P, outer == 0 && !(WLS && sp.warm), true),
+                store_partial(phase_init<V, WLS>(T, li, P, outer == 0 && !(WLS && sp.warm), true,
+                                                 zb[0]),
                               pbuf[pc & 1], T.item0 + li, sw);
             if (b > a) seg_done(T, t, b - a, pbuf[pc & 1], tbuf[pc & 1], tick, sw, &s_bcast, &s_flag);
         }
         ++pc;
-        if (!grid_sync(ctl, timeout_ns)) return;
+        if (!grid_sync(ctl, timeout_ns, !(outer == 0 && (int)blockIdx.x == sp.skip_block))) return;
 
-        /* stA: scalars after the stencil-pass decisions, stB: after the
-         * update-pass decisions; each phase reads one and writes the other,
-         * so the active flags a phase slices on never change under it */
-        TileState *stA = st, *stB = st + ntiles;
         int it = 0;
-        while (true) {
-            V *pnew = pb[(it + 1) & 1];
-            /* slice over the tiles active in the previous phase; reduce r.z,
-             * update the tile scalars, then the stencil pass */
-            setup_slice(sc, tiles, it == 0 ? nullptr : stB, ntiles, sw);
-            /* tiles not counted this phase keep their inactive flag in stA */
-            if (it > 0 && blockIdx.x == 0)
-                for (int t = threadIdx.x; t < ntiles; t += blockDim.x)
-                    if (!__ldcg(&stB[t].active)) stA[t].active = 0;
-            for (int t = sc.t0; t <= sc.t1; ++t) {
-                const TileDesc &T = stile(sc, tiles, t);
-                if (sc.pre[t + 1] == sc.pre[t]) continue;          /* not counted */
-                const bool owner = sc.pre[t] >= sc.s0 && sc.pre[t] < sc.s1;
-                TileState S;
-                if (it == 0) {
+        if constexpr (!mixed) {
+            /* ── FP64: stencil pass + update pass per iteration ──
+             * stA: scalars after the stencil-pass decisions, stB: after the
+             * update-pass decisions; each phase reads one and writes the
+             * other, so the active flags a phase slices on never change
+             * under it */
+            TileState *stA = st, *stB = st + ntiles;
+            while (true) {
+                double *pnew = (double *)pb[(it + 1) & 1];
+                /* slice over the tiles active in the previous phase; reduce
+                 * r.z, update the tile scalars, then the stencil pass */
+                setup_slice(sc, tiles, it == 0 ? nullptr : stB, ntiles, sw);
+                if (it > 0) carry_inactive(stB, stA, ntiles);
+                for (int t = sc.t0; t <= sc.t1; ++t) {
+                    const TileDesc &T = stile(sc, tiles, t);
+                    if (sc.pre[t + 1] == sc.pre[t]) continue;          /* not counted */
+                    const bool owner = sc.pre[t] >= sc.s0 && sc.pre[t] < sc.s1;
+                    TileState S;
                     double tot = __ldcg(tbuf[(pc - 1) & 1] + t);
-                    S.rz = tot;
-                    S.rz0 = tot;
-                    S.thr = (double)sp.tol * (double)sp.tol * tot;
-                    S.alpha = 0.0;
-                    S.beta = 0.0;
-                    S.iter = 0;
-                    S.active = (tot > 0.0 && sp.max_iter > 0) ? 1 : 0;
-                    if (owner && threadIdx.x == 0 && S.active) atomicAdd(&ctl->n_active, 1);
-                } else {
-                    S = load_state(stB + t);
-                    double tot = __ldcg(tbuf[(pc - 1) & 1] + t);
-                    /* a replacement iteration folded its update already */
-                    if (mixed && sp.replace_every > 0 && (it % sp.replace_every) == 0)
-                        S.alpha = 0.0;
-                    S.iter += 1;
-                    if (tot < S.thr || S.iter >= sp.max_iter) {
-                        S.active = 0;
-                        if (owner && threadIdx.x == 0) {
-                            atomicSub(&ctl->n_active, 1);
-                            atomicAdd(&ctl->px_iters, (unsigned long long)S.iter *
-                                                          (unsigned long long)((long long)T.nr * T.nc));
-                        }
+                    if (it == 0) {
+                        S = start_state(tot, sp);
+                        if (owner && threadIdx.x == 0 && S.active) atomicAdd(&ctl->n_active, 1);
                     } else {
-                        S.beta = tot / S.rz;
-                        S.rz = tot;
+                        S = load_state(stB + t);
+                        S.iter += 1;
+                        if (tot < S.thr || S.iter >= sp.max_iter) {
+                            tile_stop(S, T, owner, ctl);
+                        } else {
+                            S.beta = tot / S.rz;
+                            S.rz = tot;
+                        }
                     }
+                    put_state(sc, stA, t, S, owner);
                 }
-                if (threadIdx.x == 0) {
-                    if (owner || !scached(sc, t)) stA[t] = S;
-                    sput(sc, t, S);
-                }
-            }
-            __syncthreads();
-            run_pass<0, V>(sc, tiles, stA, ntiles, P, M, it & 1, pnew, it == 0, pbuf[pc & 1],
-                           tbuf[pc & 1], tick, sw, &s_bcast, &s_flag, Pn, dsm, bars, parity, ctl,
-                           timeout_ns);
-            ++pc;
-            if (!grid_sync(ctl, timeout_ns)) return;
-            if (*(volatile int *)&ctl->snap <= 0) break;
-
-            /* slice over the tiles active in the stencil pass; reduce p.q, alpha */
-            const bool repl = mixed && sp.replace_every > 0 && ((it + 1) % sp.replace_every) == 0;
-            setup_slice(sc, tiles, stA, ntiles, sw);
-            if (blockIdx.x == 0)
-                for (int t = threadIdx.x; t < ntiles; t += blockDim.x)
-                    if (!__ldcg(&stA[t].active)) stB[t].active = 0;
-            for (int t = sc.t0; t <= sc.t1; ++t) {
-                const TileDesc &T = stile(sc, tiles, t);
-                if (sc.pre[t + 1] == sc.pre[t]) continue;
-                const bool owner = sc.pre[t] >= sc.s0 && sc.pre[t] < sc.s1;
-                TileState S = load_state(stA + t);
-                double pq = __ldcg(tbuf[(pc - 1) & 1] + t);
-                if (pq <= 0.0) {
-                    S.active = 0;
-                    S.alpha = 0.0;
-                    if (owner && threadIdx.x == 0) {
-                        atomicSub(&ctl->n_active, 1);
-                        atomicAdd(&ctl->px_iters, (unsigned long long)S.iter *
-                                                      (unsigned long long)((long long)T.nr * T.nc));
-                    }
-                } else {
-                    S.alpha = S.rz / pq;
-                }
-                if (threadIdx.x == 0) {
-                    if (owner || !scached(sc, t)) stB[t] = S;
-                    sput(sc, t, S);
-                }
-            }
-            __syncthreads();
-            if (!repl) {
-                if (mixed)
-                    run_update_direct(sc, tiles, stB, P, pbuf[pc & 1], tbuf[pc & 1], tick, sw,
-                                      &s_bcast, &s_flag);
-                else
-                    run_pass<1, V>(sc, tiles, stB, ntiles, P, M, (it + 1) & 1, pnew, true,
-                                   pbuf[pc & 1], tbuf[pc & 1], tick, sw, &s_bcast, &s_flag, Pn, dsm,
-                                   bars, parity, ctl, timeout_ns);
-                ++pc;
-            } else {
-                /* fold this iteration's update into the FP64 solution; the
-                 * true residual follows once every neighbour has folded */
-                for (int t = sc.t0; t <= sc.t1; ++t) {
-                    const TileDesc &T = stile(sc, tiles, t);
-                    if (sc.pre[t + 1] == sc.pre[t] || !sactive(sc, stB, t)) continue;
-                    int a, b;
-                    slice_items(sc, T, t, a, b);
-                    double alpha = salpha(sc, stB, t);
-                    for (int li = a; li < b; ++li) phase_fold<V>(T, li, P, pnew, true, alpha);
-                }
-            }
-            if (!grid_sync(ctl, timeout_ns)) return;
-            if (repl) {
-                setup_slice(sc, tiles, stB, ntiles, sw);
-                for (int t = sc.t0; t <= sc.t1; ++t) {
-                    const TileDesc &T = stile(sc, tiles, t);
-                    int a, b;
-                    if (sc.pre[t + 1] == sc.pre[t]) continue;
-                    slice_items(sc, T, t, a, b);
-                    for (int li = a; li < b; ++li)
-                        store_partial(phase_init<V, WLS>(T, li, P, false, false), pbuf[pc & 1],
-                                      T.item0 + li, sw);
-                    if (b > a)
-                        seg_done(T, t, b - a, pbuf[pc & 1], tbuf[pc & 1], tick, sw, &s_bcast,
-                                 &s_flag);
-                }
+                __syncthreads();
+                run_pass<0>(sc, tiles, stA, ntiles, P, M, it & 1, pnew, it == 0, pbuf[pc & 1],
+                            tbuf[pc & 1], tick, sw, &s_bcast, &s_flag, (double *)Pn, dsm, bars,
+                            parity, ctl, timeout_ns);
                 ++pc;
                 if (!grid_sync(ctl, timeout_ns)) return;
+                if (*(volatile int *)&ctl->snap <= 0) break;
+
+                /* slice over the tiles active in the stencil pass; reduce
+                 * p.q, alpha; then the update pass */
+                setup_slice(sc, tiles, stA, ntiles, sw);
+                carry_inactive(stA, stB, ntiles);
+                for (int t = sc.t0; t <= sc.t1; ++t) {
+                    const TileDesc &T = stile(sc, tiles, t);
+                    if (sc.pre[t + 1] == sc.pre[t]) continue;
+                    const bool owner = sc.pre[t] >= sc.s0 && sc.pre[t] < sc.s1;
+                    TileState S = load_state(stA + t);
+                    double pq = __ldcg(tbuf[(pc - 1) & 1] + t);
+                    if (pq <= 0.0) {
+                        tile_stop(S, T, owner, ctl);
+                        S.alpha = 0.0;
+                    } else {
+                        S.alpha = S.rz / pq;
+                    }
+                    put_state(sc, stB, t, S, owner);
+                }
+                __syncthreads();
+                run_pass<1>(sc, tiles, stB, ntiles, P, M, (it + 1) & 1, pnew, true, pbuf[pc & 1],
+                            tbuf[pc & 1], tick, sw, &s_bcast, &s_flag, (double *)Pn, dsm, bars,
+                            parity, ctl, timeout_ns);
+                ++pc;
+                if (!grid_sync(ctl, timeout_ns)) return;
+                ++it;
             }
-            ++it;
-        }
-        if (mixed) {
-            /* fold the FP32 increments of the pass into the FP64 solution,
-             * with each tile's deferred last update: a tile that stopped in
-             * an r.z reduction at iteration i (stA.iter = i, stB.iter = i-1)
-             * still owes alpha_{i-1} p_{i-1} (p in pb[i & 1]; alpha zeroed
-             * when a replacement fold applied it); one that stopped in a p.q
-             * reduction (stA.iter = stB.iter) owes nothing */
+        } else {
+            /* ── mixed: one pass per iteration ──
+             * Before pass k the tile scalars take the totals of the last
+             * reduction: after a pass that updated z, its true r.z (stop
+             * test), then alpha_{k-1} = r.z / p.q and the recurrence for
+             * beta_k; after a true-residual assembly, its r.z.  Each such
+             * step reads st[cur] and writes st[cur ^ 1]. */
+            float *qb[2] = {(float *)P.q, P.q1};
+            int zsel = 0, cur = 0;
+            bool prev_fresh = true;
+            for (int k = 0;; ++k) {
+                const bool repl = k > 0 && sp.replace_every > 0 && (k % sp.replace_every) == 0;
+                {
+                    TileState *sP = st + (size_t)cur * ntiles, *sN = st + (size_t)(cur ^ 1) * ntiles;
+                    setup_slice(sc, tiles, k == 0 ? nullptr : sP, ntiles, sw);
+                    if (k > 0) carry_inactive(sP, sN, ntiles);
+                    const double *tt = tbuf[(pc - 1) & 1];
+                    for (int t = sc.t0; t <= sc.t1; ++t) {
+                        const TileDesc &T = stile(sc, tiles, t);
+                        if (sc.pre[t + 1] == sc.pre[t]) continue;
+                        const bool owner = sc.pre[t] >= sc.s0 && sc.pre[t] < sc.s1;
+                        TileState S;
+                        if (k == 0) {
+                            S = start_state(__ldcg(tt + t), sp);
+                            if (owner && threadIdx.x == 0 && S.active) atomicAdd(&ctl->n_active, 1);
+                        } else {
+                            S = load_state(sP + t);
+                            if (!prev_fresh) {
+                                const double rz = __ldcg(tt + t);
+                                S.iter += 1;
+                                if (rz < S.thr || S.iter >= sp.max_iter) tile_stop(S, T, owner, ctl);
+                                else S.rz = rz;
+                            }
+                            if (S.active) {
+                                const double pq = __ldcg(tt + (size_t)ntiles + t);
+                                if (pq <= 0.0) {
+                                    tile_stop(S, T, owner, ctl);
+                                    S.alpha = 0.0;
+                                } else {
+                                    S.alpha = S.rz / pq;
+                                    const double zq = __ldcg(tt + 2 * (size_t)ntiles + t);
+                                    const double qq = __ldcg(tt + 3 * (size_t)ntiles + t);
+                                    const double rzn = __fma_rn(S.alpha * S.alpha, qq,
+                                                                __fma_rn(-2.0 * S.alpha, zq, S.rz));
+                                    S.beta = rzn > 0.0 ? rzn / S.rz : 0.0;
+                                }
+                            }
+                        }
+                        put_state(sc, sN, t, S, owner);
+                    }
+                    __syncthreads();
+                    cur ^= 1;
+                }
+                bool fresh = k == 0;
+                if (repl) {
+                    /* fold x += dx + alpha_{k-1} p_{k-1} (dx = 0), then the true
+                     * residual b - A x replaces the recursive one */
+                    const TileState *sC = st + (size_t)cur * ntiles;
+                    for (int t = sc.t0; t <= sc.t1; ++t) {
+                        const TileDesc &T = stile(sc, tiles, t);
+                        if (sc.pre[t + 1] == sc.pre[t] || !sactive(sc, sC, t)) continue;
+                        int a, b;
+                        slice_items(sc, T, t, a, b);
+                        const double alpha = salpha(sc, sC, t);
+                        for (int li = a; li < b; ++li)
+                            phase_fold<float>(T, li, P, (const float *)pb[k & 1], true, alpha);
+                    }
+                    if (!grid_sync(ctl, timeout_ns)) return;
+                    setup_slice(sc, tiles, sC, ntiles, sw);
+                    for (int t = sc.t0; t <= sc.t1; ++t) {
+                        const TileDesc &T = stile(sc, tiles, t);
+                        if (sc.pre[t + 1] == sc.pre[t]) continue;
+                        int a, b;
+                        slice_items(sc, T, t, a, b);
+                        for (int li = a; li < b; ++li)
+                            store_partial(phase_init<V, WLS>(T, li, P, false, false, zb[zsel]),
+                                          pbuf[pc & 1], T.item0 + li, sw);
+                        if (b > a)
+                            seg_done(T, t, b - a, pbuf[pc & 1], tbuf[pc & 1], tick, sw, &s_bcast,
+                                     &s_flag);
+                    }
+                    ++pc;
+                    if (!grid_sync(ctl, timeout_ns)) return;
+                    /* stop test on the true r.z, beta from it */
+                    TileState *sP = st + (size_t)cur * ntiles, *sN = st + (size_t)(cur ^ 1) * ntiles;
+                    setup_slice(sc, tiles, sP, ntiles, sw);
+                    carry_inactive(sP, sN, ntiles);
+                    for (int t = sc.t0; t <= sc.t1; ++t) {
+                        const TileDesc &T = stile(sc, tiles, t);
+                        if (sc.pre[t + 1] == sc.pre[t]) continue;
+                        const bool owner = sc.pre[t] >= sc.s0 && sc.pre[t] < sc.s1;
+                        TileState S = load_state(sP + t);
+                        const double rz = __ldcg(tbuf[(pc - 1) & 1] + t);
+                        S.iter += 1;
+                        if (rz < S.thr || S.iter >= sp.max_iter) {
+                            tile_stop(S, T, owner, ctl);
+                        } else {
+                            S.beta = rz / S.rz;
+                            S.rz = rz;
+                        }
+                        S.alpha = 0.0;
+                        put_state(sc, sN, t, S, owner);
+                    }
+                    __syncthreads();
+                    cur ^= 1;
+                    fresh = true;
+                }
+                run_pass_s(sc, tiles, st + (size_t)cur * ntiles, ntiles, nitems, M, zsel, k & 1,
+                           k == 0, fresh, (float *)pb[(k + 1) & 1], (float *)zb[zsel ^ 1],
+                           qb[(k + 1) & 1], P.dx, pbuf[pc & 1], tbuf[pc & 1], tick, sw, sw4,
+                           &s_bcast, &s_flag, (float *)Pn, dsm, bars, parity, ctl, timeout_ns);
+                ++pc;
+                if (!fresh) zsel ^= 1;
+                prev_fresh = fresh;
+                if (!grid_sync(ctl, timeout_ns)) return;
+                if (*(volatile int *)&ctl->snap <= 0) break;
+            }
+            /* fold the FP32 increments of the pass into the FP64 solution
+             * (every update has been applied to dx by then) */
             setup_slice(sc, tiles, nullptr, ntiles, sw);
             for (int t = sc.t0; t <= sc.t1; ++t) {
                 const TileDesc &T = stile(sc, tiles, t);
                 int a, b;
                 slice_items(sc, T, t, a, b);
-                if (a >= b) continue;
-                const int ia = __ldcg(&stA[t].iter), ib = __ldcg(&stB[t].iter);
-                const double ap = ia == ib ? 0.0 : __ldcg(&stA[t].alpha);
-                const V *pl = pb[ia & 1];
-                for (int li = a; li < b; ++li) phase_fold<V>(T, li, P, pl, ap != 0.0, ap);
+                for (int li = a; li < b; ++li) phase_fold<float>(T, li, P, nullptr, false, 0.0);
             }
             if (!grid_sync(ctl, timeout_ns)) return;
+            it = *(volatile int *)&ctl->pass_max;
         }
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             if (sp.pass_iters) sp.pass_iters[outer] = it;
             ctl->total_iters += it;
             if (it > ctl->max_pass_iters) ctl->max_pass_iters = it;
+            ctl->pass_max = 0;
         }
         if (outer < sp.n_irls) {
             float delta = sp.deltas[outer];
@@ -1379,21 +1615,27 @@ static int make_map(CUtensorMap &m, const void *base, size_t esize, int pitch, i
 template <typename V>
 static int make_maps(SolveMaps &M, const SolverPlanes &P, int pitch, int rows)
 {
-    const size_t v = sizeof(V);
     int rc = 0;
-    rc |= make_map(M.zA, P.z, v, pitch, rows, kSegW, kItemBy + 2);
-    rc |= make_map(M.p0A, P.p0, v, pitch, rows, kSegW, kItemBy + 2);
-    rc |= make_map(M.p1A, P.p1, v, pitch, rows, kSegW, kItemBy + 2);
-    rc |= make_map(M.wdA, P.wd, 4, pitch, rows, kItemBx, kItemBy + 1);
-    rc |= make_map(M.wrA, P.wr, 4, pitch, rows, kWrW, kItemBy);
-    if (v == 4) rc |= make_map(M.xB, P.dx, 4, pitch, rows, kItemBx, kItemBy);
-    else rc |= make_map(M.xB, P.x, 8, pitch, rows, kItemBx, kItemBy);
-    rc |= make_map(M.zB, P.z, v, pitch, rows, kItemBx, kItemBy);
-    rc |= make_map(M.p0B, P.p0, v, pitch, rows, kItemBx, kItemBy);
-    rc |= make_map(M.p1B, P.p1, v, pitch, rows, kItemBx, kItemBy);
-    rc |= make_map(M.qB, P.q, v, pitch, rows, kItemBx, kItemBy);
-    rc |= make_map(M.rB, v == 8 ? P.r : P.z, v, pitch, rows, kItemBx, kItemBy);
-    rc |= make_map(M.dB, P.diag, v, pitch, rows, kItemBx, kItemBy);
+    rc |= make_map(M.zA, P.z, sizeof(V), pitch, rows, kSegW, kItemBy + 2);
+    rc |= make_map(M.p0A, P.p0, sizeof(V), pitch, rows, kSegW, kItemBy + 2);
+    rc |= make_map(M.p1A, P.p1, sizeof(V), pitch, rows, kSegW, kItemBy + 2);
+    if (sizeof(V) == 8) {
+        rc |= make_map(M.wdA, P.wd, 4, pitch, rows, kItemBx, kItemBy + 1);
+        rc |= make_map(M.wrA, P.wr, 4, pitch, rows, kWrW, kItemBy);
+        rc |= make_map(M.xB, P.x, 8, pitch, rows, kItemBx, kItemBy);
+        rc |= make_map(M.p0B, P.p0, 8, pitch, rows, kItemBx, kItemBy);
+        rc |= make_map(M.p1B, P.p1, 8, pitch, rows, kItemBx, kItemBy);
+        rc |= make_map(M.qB, P.q, 8, pitch, rows, kItemBx, kItemBy);
+        rc |= make_map(M.rB, P.r, 8, pitch, rows, kItemBx, kItemBy);
+        rc |= make_map(M.dB, P.diag, 8, pitch, rows, kItemBx, kItemBy);
+    } else {
+        rc |= make_map(M.zS1, P.r, 4, pitch, rows, kSegW, StageS::kBoxH);
+        rc |= make_map(M.qS0, P.q, 4, pitch, rows, kSegW, StageS::kBoxH);
+        rc |= make_map(M.qS1, P.q1, 4, pitch, rows, kSegW, StageS::kBoxH);
+        rc |= make_map(M.wdS, P.wd, 4, pitch, rows, kSegW, StageS::kWdH);
+        rc |= make_map(M.wrS, P.wr, 4, pitch, rows, kSegW, StageS::kBoxH);
+        rc |= make_map(M.xB, P.dx, 4, pitch, rows, kItemBx, kItemBy);
+    }
     return rc ? CUPHU_ERR_CUDA : 0;
 }
 
@@ -1406,6 +1648,7 @@ static int launch_solve_kernel(const TileDesc *tiles, const int *item_tile, int 
     if (ntiles > kMaxTiles)
         return fail(CUPHU_ERR_INVALID, "at most 1024 tiles per solver launch");
     SolveMaps M;
+    std::memset(&M, 0, sizeof(M));
     int rcm = make_maps<V>(M, P, pitch, rows);
     if (rcm) return rcm;
     int nsm = 0, per_sm = 0;
@@ -1449,11 +1692,24 @@ static int launch_solve_t(const TileDesc *tiles, const int *item_tile, int nitem
                                          ctl, sp, timeout_ns, device, s);
 }
 
+/* the failure test's one-shot switch, per device */
+static std::atomic<int> g_skip_block[64];
+static std::once_flag g_skip_init;
+
+void solver_skip_barrier_once(int dev, int block)
+{
+    std::call_once(g_skip_init, [] { for (auto &v : g_skip_block) v.store(-1); });
+    if (dev >= 0 && dev < 64) g_skip_block[dev].store(block);
+}
+
 int launch_solve(bool fp64, const TileDesc *tiles, const int *item_tile, int nitems,
                  int ntiles, const SolverPlanes &P, int plane_pitch, int plane_rows,
-                 TileState *st, double *part, SolverCtl *ctl, const SolveParams &sp,
+                 TileState *st, double *part, SolverCtl *ctl, const SolveParams &sp_in,
                  int device, cudaStream_t s)
 {
+    std::call_once(g_skip_init, [] { for (auto &v : g_skip_block) v.store(-1); });
+    SolveParams sp = sp_in;
+    if (device >= 0 && device < 64) sp.skip_block = g_skip_block[device].exchange(-1);
     long long timeout_ns = sp.timeout_ns;
     if (fp64)
         return launch_solve_t<double>(tiles, item_tile, nitems, ntiles, P, plane_pitch, plane_rows,

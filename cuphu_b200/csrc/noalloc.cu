@@ -20,7 +20,9 @@
  * In host code the array's name is only a host-side stand-in for the device
  * symbol.  Its device address is looked up once per device, with that device
  * current, by cudaGetSymbolAddress, the first time the entry point runs on
- * that device.  Make that first call before any stream capture begins.
+ * that device.  Make that first call before any stream capture begins.  The
+ * address is kept for the life of the process: it does not survive a
+ * cudaDeviceReset, after which the library's module is loaded anew.
  *
  * Every call on a device shares the one array, and the array keeps the last
  * call's contents.  No element has to start at zero: k_int_rowoff writes rows

@@ -214,6 +214,39 @@ __global__ void __launch_bounds__(256) k_merge(const ScenePlan *__restrict__ sce
     }
 }
 
+/* the reference-pixel shift of a merged scene whose post-passes ran after
+ * the merge: n = rint((unw[ref] - phi[ref]) / 2pi), then unw -= float(n 2pi)
+ * (the merge kernel's rule, on the post-processed value) */
+__global__ void k_ref_shift_n(const float *unw, const float *ph, int ncol, int ref_row,
+                              int ref_col, SceneOut *o)
+{
+    size_t i = (size_t)ref_row * ncol + ref_col;
+    double n = rint(((double)unw[i] - (double)ph[i]) / kTwoPiD);
+    o->shift = (float)(n * kTwoPiD);
+    o->do_shift = n != 0.0 ? 1 : 0;
+}
+
+__global__ void __launch_bounds__(256) k_ref_shift_apply(float *unw, long long n,
+                                                         const SceneOut *o)
+{
+    if (!o->do_shift) return;
+    const float sh = o->shift;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        unw[i] = unw[i] - sh;
+}
+
+int launch_ref_shift(float *unw, const float *ph, int nrow, int ncol, int ref_row, int ref_col,
+                     SceneOut *tmp, cudaStream_t s)
+{
+    if (ref_row < 0 || ref_col < 0 || ref_row >= nrow || ref_col >= ncol) return 0;
+    k_ref_shift_n<<<1, 1, 0, s>>>(unw, ph, ncol, ref_row, ref_col, tmp);
+    long long n = (long long)nrow * ncol;
+    int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+    k_ref_shift_apply<<<blocks, 256, 0, s>>>(unw, n, tmp);
+    return cuda_fail(cudaGetLastError(), "reference-pixel shift");
+}
+
 int launch_stitch(const ScenePlan *scenes, int nscenes, const TileDesc *tiles,
                   const PairDesc *pairs, int npairs, const SolverPlanes &P,
                   const int *ntile_labels, double *pair_k, double *tile_k,

@@ -89,8 +89,8 @@ typedef struct CuPhuTileParams {
     int fix_cycle_spikes;
 } CuPhuTileParams;
 
-/* ref cuphu.h:142-162 -- identical layout; bridging is not part of this
- * build, enabled != 0 returns CUPHU_ERR_UNSUPPORTED */
+/* ref cuphu.h:142-162 -- identical layout; enabled != 0 runs phase
+ * bridging as the last stage of cuphu_unwrap */
 typedef enum {
     CUPHU_RAMP_NONE = 0, CUPHU_RAMP_LINEAR, CUPHU_RAMP_QUADRATIC,
     CUPHU_RAMP_LINEAR_RANGE, CUPHU_RAMP_LINEAR_AZIMUTH,
@@ -129,6 +129,15 @@ typedef struct CuPhuSolveOptions {
     int   replace_every;      /* mixed: true-residual replacement period (50)    */
     int   ref_row, ref_col;   /* reference pixel; -1 disables the 2pi shift      */
     int   timeout_ms;         /* device spin limit per grid barrier (5000)       */
+    int   device_phase;       /* host-buffer entry points: 0 = wrapped phase from
+                                 the host C library's float atan2, as the reference
+                                 computes it (bit-exact downstream; default),
+                                 1 = the device's correctly rounded angle        */
+    int   merge_conncomp;     /* multi-tile scenes: 0 = per-tile label spaces
+                                 offset tile by tile, as the reference merges
+                                 them (default); 1 = one labelling of the whole
+                                 stitched scene, so components that cross tile
+                                 seams get one label                            */
 } CuPhuSolveOptions;
 
 /* per-call statistics (new) */
@@ -325,12 +334,89 @@ int cuphu_integrate_phase_gpu(const float *wrapped_phase, const short *hflows,
  * the library (CUPHU_NOALLOC_MAX_ROWS floats, held by every GPU that loads
  * the library until exit), so nrow above CUPHU_NOALLOC_MAX_ROWS returns
  * CUPHU_ERR_INVALID.  The first call on a device looks up the array's
- * device address: make it before any stream capture.  All calls on a
- * device share the array, so calls that overlap on the GPU race; order
- * them on one stream or with events. */
+ * device address: make it before any stream capture.  The address is kept
+ * for the life of the process and does not survive cudaDeviceReset.  All
+ * calls on a device share the array, so calls that overlap on the GPU race;
+ * order them on one stream or with events. */
 #define CUPHU_NOALLOC_MAX_ROWS 65536
 int cuphu_integrate_phase_noalloc(const float *wrapped_phase, const short *hflows,
                                   const short *vflows, int nrow, int ncol, float *unw_out,
+                                  void *stream);
+
+/* ── a scene fed band by band (new; the reference reads its inputs whole,
+ *    _unwrap.py:515-523).  create: device planes for an nrow x ncol scene
+ *    on gpu_id; flags say which masks the bands carry.  put_rows: host
+ *    buffers of rows [row0, row0+nrows) (igram as interleaved complex64);
+ *    the reference's host phase of the band is computed on the calling
+ *    thread and the band is copied into one of two pinned staging slots and
+ *    uploaded asynchronously, so the caller can read the next band while this
+ *    one is in flight (the caller's buffers may be reused on return).
+ *    unwrap: once every row has been put, the pipeline of cuphu_unwrap_device
+ *    on the resident scene (synchronous).  get_rows: rows of the outputs into
+ *    host buffers (either may be NULL).  destroy: frees the handle. */
+#define CUPHU_STREAM_MASK      1   /* bands carry the solve mask           */
+#define CUPHU_STREAM_ORIG_MASK 2   /* bands carry the original mask        */
+int cuphu_stream_create(int nrow, int ncol, int flags, int gpu_id, void **handle);
+int cuphu_stream_put_rows(void *handle, int row0, int nrows, const float *igram_c64,
+                          const float *corr, const unsigned char *mask,
+                          const unsigned char *orig_mask);
+int cuphu_stream_unwrap(void *handle, CuPhuCostMode cost_mode, const CuPhuParams *params,
+                        const CuPhuTileParams *tile, const CuPhuSolveOptions *opts,
+                        CuPhuSolveStats *stats);
+int cuphu_stream_get_rows(void *handle, int row0, int nrows, float *unw_out,
+                          uint32_t *conncomp_out);
+int cuphu_stream_destroy(void *handle);
+
+/* ── inputs of the CPU network-flow front end, computed on the GPU (new;
+ *    the reference computes them on the host, cuphu_solver.cpp:513-633).
+ * cuphu_mst_costs_device: initial-flow arc weights of SMOOTH costs (device
+ * smoothcostT pairs, flat row-then-col layout): SNAPHU's incremental cost of
+ * a +-1 flow from flow 0, w = clip(min(pos, neg), 1, maxcost).
+ * cuphu_mcf_inputs: host buffers; the reference's host phase, the cost
+ * arrays (costs_out: 2 shorts per arc for SMOOTH, 4 for DEFO/TOPO), their
+ * initial-flow weights (mst_costs_out, narcs shorts, SMOOTH only; NULL to
+ * skip) and the residues (residues_out, (nrow-1)*(ncol-1), NULL to skip),
+ * one host-to-device copy in and one device-to-host copy per output. */
+int cuphu_mst_costs_device(const void *d_smooth_costs, long long narcs, long nshortcycle,
+                           long maxcost, short *d_out, void *stream);
+int cuphu_mcf_inputs(const float *igram_r, const float *igram_i, const float *corr,
+                     const short *weights, int nrow, int ncol, CuPhuCostMode cost_mode,
+                     const CuPhuParams *params, int gpu_id, short *costs_out,
+                     short *mst_costs_out, signed char *residues_out);
+
+/* ── phase bridging (ref cuphu_solver.cpp:996-1352, cuphu_bridge_gpu.cu):
+ * whole-cycle offsets between the 8-connected regions of nonzero, unmasked
+ * pixels (regions under min_num_pixel or without an erosion survivor
+ * dropped) are reconciled along the minimum spanning tree of their nearest
+ * boundary points from the largest region, by window medians of radius
+ * `radius`, with an optional ramp (ramp_type) removed over the largest
+ * region first.  conncomp is overwritten with the region labels.  Some
+ * stages synchronise the stream.  Nothing changes when fewer than two
+ * regions remain.
+ * ref cuphu.h:381-389 (void there): host buffers, gpu_id selects the device */
+int cuphu_bridge_apply_test(float *unw, uint32_t *conncomp, int nrow, int ncol,
+                            const CuPhuBridgeParams *bridge, const unsigned char *mask,
+                            int gpu_id);
+/* new: device buffers on `stream` of the current device */
+int cuphu_bridge_device(float *d_unw, uint32_t *d_conncomp, const unsigned char *d_mask, int nrow,
+                        int ncol, const CuPhuBridgeParams *bridge, void *stream);
+
+/* ── optional post-passes on a stitched scene (ref cuphu_solver.cpp
+ *    :1385-1441, 1469-1656).  The pipeline runs them after the tile merge
+ *    of a multi-tile scene when CuPhuTileParams.laplace_neighbor_feedback /
+ *    fix_cycle_spikes are set (feedback first), before the reference-pixel
+ *    shift.  mask (0 = invalid) may be NULL.  */
+/* ref cuphu.h:397-409 (void there); host buffers, unw updated in place */
+int cuphu_laplace_neighbor_feedback_test(float *unw, const unsigned char *mask, int nrow,
+                                         int ncol, int ntr, int ntc, int row_ovrlp,
+                                         int col_ovrlp, int feather_px);
+/* ref cuphu.h:415-420 (void there); host buffers, unw updated in place */
+int cuphu_fix_cycle_spikes_test(float *unw, const unsigned char *mask, int nrow, int ncol);
+/* new: the same on device buffers, asynchronous on `stream` */
+int cuphu_laplace_neighbor_feedback_device(float *d_unw, const unsigned char *d_mask, int nrow,
+                                           int ncol, int ntr, int ntc, int row_ovrlp,
+                                           int col_ovrlp, int feather_px, void *stream);
+int cuphu_fix_cycle_spikes_device(float *d_unw, const unsigned char *d_mask, int nrow, int ncol,
                                   void *stream);
 
 /* ── connected components (ref cuphu.h:275-289, cuphu_conncomp.cu:290-428) */
@@ -355,6 +441,13 @@ int cuphu_gpu_count(void);
 int cuphu_gpu_name(int device, char *buf, int len);
 int cuphu_gpu_info(int device, long long *total_memory, int *sm_count, int *cc_major,
                    int *cc_minor);
+
+/* test hook (new): the next persistent solve launched on gpu_id runs with
+ * block `block` not arriving at its first grid barrier, so every block's
+ * bounded wait runs out after CuPhuSolveOptions.timeout_ms and the call's
+ * device status becomes CUPHU_ERR_TIMEOUT (read by cuphu_last_status, or
+ * returned by calls that wait).  One-shot: later launches are normal. */
+int cuphu_test_skip_barrier_once(int gpu_id, int block);
 
 /* wait for the last pipeline enqueued on a device and return its device-side
  * status (CUPHU_ERR_TIMEOUT when a grid barrier gave up) (new) */

@@ -108,7 +108,7 @@ def test_unwrap_validation():
     with pytest.raises(NotImplementedError, match="laplace"):
         cuphu.unwrap(ig, corr, 10.0, init="mcf")
     with pytest.raises(NotImplementedError):
-        cuphu.unwrap(ig, corr, 10.0, init="laplace", bridge=True)
+        cuphu.unwrap(ig, corr, 10.0, init="laplace", single_tile_reoptimize=True)
     with pytest.raises(ValueError, match="precision"):
         cuphu.unwrap(ig, corr, 10.0, init="laplace", precision="fp16")
 

@@ -61,6 +61,15 @@ def _oracle_unwrap(ig, corr, mask, orig_mask, nrow, ncol, cost, params, tile, n_
                              kperp=params.kperpdpsi, kpar=params.kpardpsi,
                              minfrac=params.minconncompfrac, maxncomps=params.maxncomps,
                              conncompthresh=params.conncompthresh)
+    # the library's post-passes on multi-tile scenes (feedback, then spikes)
+    if tile.ntilerow * tile.ntilecol > 1:
+        m2 = None if mask is None else mask.reshape(nrow, ncol)
+        if tile.laplace_neighbor_feedback:
+            u = O.neighbor_feedback(u, (tile.ntilerow, tile.ntilecol),
+                                    (tile.rowovrlp, tile.colovrlp),
+                                    tile.laplace_neighbor_feedback_feather, m2)
+        if tile.fix_cycle_spikes:
+            u = O.fix_cycle_spikes(u, m2)
     return u, c
 
 
@@ -88,6 +97,11 @@ class StandIn:
         om = None if not orig_mask else _host(orig_mask, n, C.c_uint8).copy()
         u, c = _oracle_unwrap(ig, _host(corr, n, C.c_float).copy(), m, om, nrow, ncol, cost,
                               _struct(params), _struct(tile), self.N_IRLS)
+        b = _struct(bridge) if bridge else None
+        if b is not None and b.enabled:
+            u, c = O.bridge(u, m.reshape(nrow, ncol) if m is not None else None, b.radius,
+                            b.min_num_pixel, b.erosion_size, b.max_boundary_samples,
+                            O.RAMPS[b.ramp_type], b.ramp_max_num_sample)
         res = _struct(result)
         pu, pc = _libc.malloc(4 * n), _libc.malloc(4 * n)
         C.memmove(pu, u.ctypes.data, 4 * n)
@@ -96,6 +110,32 @@ class StandIn:
         res.conncomp = C.cast(pc, C.POINTER(C.c_uint32))
         res.nrow, res.ncol = nrow, ncol
         self.calls.append(("cuphu_unwrap", _struct(tile).ntilerow, _struct(tile).ntilecol))
+        return 0
+
+    def cuphu_bridge_apply_test(self, unw, cc, nrow, ncol, bridge, mask, gpu_id):
+        n = nrow * ncol
+        u = _host(unw, n, C.c_float)
+        c = _host(cc, n, C.c_uint32)
+        m = None if not mask else _host(mask, n, C.c_uint8).reshape(nrow, ncol).copy()
+        b = _struct(bridge)
+        ou, oc = O.bridge(u.reshape(nrow, ncol).copy(), m, b.radius, b.min_num_pixel,
+                          b.erosion_size, b.max_boundary_samples, O.RAMPS[b.ramp_type],
+                          b.ramp_max_num_sample)
+        if oc.any():      # bridging ran: both outputs replaced
+            u[:] = ou.ravel()
+            c[:] = oc.ravel()
+        self.calls.append(("bridge_hook",))
+        return 0
+
+    def cuphu_laplace_neighbor_feedback_test(self, unw, mask, nrow, ncol, ntr, ntc, rovl, covl,
+                                             feather):
+        n = nrow * ncol
+        u = _host(unw, n, C.c_float)
+        m = None if not mask else _host(mask, n, C.c_uint8).reshape(nrow, ncol).copy()
+        out = O.neighbor_feedback(u.reshape(nrow, ncol).copy(), (ntr, ntc), (rovl, covl), feather,
+                                  m)
+        u[:] = out.ravel()
+        self.calls.append(("feedback_hook", ntr, ntc))
         return 0
 
     def cuphu_unwrap_ex(self, igram, corr, mask, orig_mask, nrow, ncol, cost, params, tile, opts,
@@ -148,6 +188,17 @@ CASES = {
     "tiles_2x2": dict(cost="smooth", ntiles=(2, 2), tile_overlap=16, target_tile_size=64),
     "mask_pad": dict(cost="smooth", mask_pad_distance=3),
     "nan_samples": dict(cost="topo"),
+    "feedback": dict(cost="defo", ntiles=(2, 2), tile_overlap=16,
+                     laplace_neighbor_feedback=True, laplace_neighbor_feedback_feather=30),
+    "feedback_mask_pad": dict(cost="smooth", ntiles=(1, 2), tile_overlap=20, mask_pad_distance=2,
+                              laplace_neighbor_feedback=True,
+                              laplace_neighbor_feedback_feather=25),
+    "spikes": dict(cost="smooth", ntiles=(2, 1), tile_overlap=12, fix_cycle_spikes=True),
+    "bridge": dict(cost="defo", bridge=True, bridge_radius=30, bridge_min_num_pixel=20,
+                   bridge_erosion_size=1),
+    "bridge_ramp_shift": dict(cost="smooth", ntiles=(1, 2), tile_overlap=16, bridge=True,
+                              bridge_radius=25, bridge_erosion_size=0,
+                              bridge_ramp_type="linear", reference_pixel=(3, 100)),
 }
 
 
@@ -158,7 +209,7 @@ def test_reference_unwrap_py_runs_on_this_extension(ref, case):
     ig, g = _scene()
     kw = dict(CASES[case])
     kw["n_irls"] = StandIn.N_IRLS
-    if case == "mask_pad":
+    if case in ("mask_pad", "feedback_mask_pad", "bridge", "bridge_ramp_shift"):
         mask = np.ones(g.shape, np.uint8)
         mask[30:40, 20:90] = 0
         kw["mask"] = mask
@@ -167,14 +218,24 @@ def test_reference_unwrap_py_runs_on_this_extension(ref, case):
         g = g.copy()
         ig[5, 7] = np.nan
         g[11, 13] = np.inf
+    if case.startswith("bridge"):
+        kw["mask"][:, 50:53] = 0          # splits the scene into two regions
+    kw.setdefault("reference_pixel", None)
     ref_kw = {k: v for k, v in kw.items() if k != "n_irls"}
-    u_ref, c_ref = pkg.unwrap(ig, g, 5.0, init="laplace", reference_pixel=None, **ref_kw)
+    u_ref, c_ref = pkg.unwrap(ig, g, 5.0, init="laplace", **ref_kw)
+    n_ref = len(stand.calls)
     u_out = np.zeros(g.shape, np.float32)
     c_out = np.zeros(g.shape, np.uint32)
-    u, c = cuphu_b200.unwrap(ig, g, 5.0, init="laplace", reference_pixel=None, unw=u_out,
-                             conncomp=c_out, **kw)
+    u, c = cuphu_b200.unwrap(ig, g, 5.0, init="laplace", unw=u_out, conncomp=c_out, **kw)
     assert u is u_out and c is c_out
-    assert [x[1:] for x in stand.calls[0::2]] == [x[1:] for x in stand.calls[1::2]]
+    # the same library calls in the same order: one unwrap (split-plane or
+    # interleaved entry point), then the boundary hook when it is needed
+    def norm(calls):
+        return [("unwrap" if c[0].startswith("cuphu_unwrap") else c[0],) + tuple(c[1:])
+                for c in calls if c[0] != "bridge_hook"]
+    assert norm(stand.calls[:n_ref]) == norm(stand.calls[n_ref:])
+    if case.startswith("bridge"):
+        assert c_ref.max() == 2           # the two bridged regions label the scene
     assert u_ref.dtype == np.float32 and c_ref.dtype == np.uint32
     assert np.array_equal(u.view(np.int32), u_ref.view(np.int32))
     assert np.array_equal(c, c_ref)
@@ -219,11 +280,12 @@ def test_validation_errors_match_the_reference(ref, bad):
 def test_unsupported_options_raise_instead_of_being_dropped(ref):
     pkg, _ = ref
     ig, g = _scene(20, 24)
-    for opt in ("single_tile_reoptimize", "fix_cycle_spikes", "bridge"):
-        with pytest.raises(NotImplementedError):
-            pkg.unwrap(ig, g, 5.0, init="laplace", **{opt: True})
     with pytest.raises(NotImplementedError):
-        _cuphu_ext.unwrap_arrays(ig, g, 5.0, init="laplace", laplace_neighbor_feedback=True)
+        pkg.unwrap(ig, g, 5.0, init="laplace", single_tile_reoptimize=True)
+    with pytest.raises(NotImplementedError):
+        _cuphu_ext.unwrap_arrays(ig, g, 5.0, init="laplace", single_tile_reoptimize=True)
+    with pytest.raises(ValueError, match="bridge_ramp_type"):
+        _cuphu_ext.unwrap_arrays(ig, g, 5.0, init="laplace", bridge=True, bridge_ramp_type="x")
     with pytest.raises(ValueError, match="cost must be"):
         _cuphu_ext.unwrap_arrays(ig, g, 5.0, cost="nope")
     with pytest.raises(RuntimeError, match="2-D"):
