@@ -85,7 +85,8 @@ struct CostConsts {
     float nsc_f;          /* nshortcycle (exact in float) */
     float thr_lo, thr_hi; /* coherence threshold bracket, 2^-20 relative */
     float a_f, c_f;       /* v = a_f b^rhopow + c_f (weight 1) */
-    float m_off;          /* offset rounding margin */
+    float off_hm;         /* 1/2 - offset rounding margin (rounded down) */
+    float half_m;         /* 1/2 - 1e-6 (rounded down): sigsq margin base */
     int s_rho0;           /* truncated sigsq of a zero-coherence arc, weight 1 */
 };
 

@@ -64,7 +64,9 @@ CostConsts make_cost_consts(const CuPhuParams &p)
     k.thr_hi = std::nextafter((float)(k.thresh * (1.0 + std::ldexp(1.0, -20))), 3.0e38f);
     k.a_f = (float)(k.sigsqrhoconst * k.nsc2 / k.costscale);
     k.c_f = (float)(k.sigsqcorr * k.nsc2 / k.costscale);
-    k.m_off = (float)(std::fabs(k.nsc) * std::ldexp(1.0, -22) + std::ldexp(1.0, -30));
+    const double m_off = std::fabs(k.nsc) * std::ldexp(1.0, -22) + std::ldexp(1.0, -30);
+    k.off_hm = std::nextafter((float)(0.5 - m_off), 0.0f);
+    k.half_m = std::nextafter((float)(0.5 - 1e-6), 0.0f);
     /* the reference's FP64 arithmetic at rho = 0 (pow(1, rhopow) = 1) */
     double t0 = std::fma(k.sigsqrhoconst, 1.0, k.sigsqcorr);
     t0 = t0 * k.nsc2;
@@ -77,6 +79,8 @@ CostConsts make_cost_consts(const CuPhuParams &p)
                     std::isfinite(k.rhopow) && k.rhopow > 0.0 && k.rhopow < 64.0 &&
                     std::isfinite(k.thresh) && k.thresh > 0.0 && k.thresh < 1.0 &&
                     std::isfinite(k.a_f) && std::isfinite(k.c_f) && k.s_rho0 >= 0 &&
+                    /* v = a b^rhopow + c < 1e6 for every b in [0, 1] */
+                    ((double)k.a_f * 1.001 + (double)k.c_f) * 1.001 < 1.0e6 &&
                     std::isfinite(k.nsc2);
     k.fast = ok ? 1 : 0;
     return k;
@@ -513,62 +517,73 @@ __device__ __forceinline__ float ex2_ftz(float x)
     return y;
 }
 
+/* coherence as the FP32 fast path reads it: values in [0, 1] unchanged,
+ * non-finite values as 0 (sane), and every other value -- finite outside
+ * [0, 1], or -0 -- as NaN.  A NaN fails the threshold test of arc_lane, so
+ * the arc goes to the exact arithmetic, which reloads the stored value. */
+__device__ __forceinline__ float cor_fast(float c)
+{
+    const unsigned u = __float_as_uint(c);
+    if (u <= 0x3f800000u) return c;
+    return (u & 0x7fffffffu) >= 0x7f800000u ? 0.0f : __uint_as_float(0x7fc00000u);
+}
+
 /* arc_lane / arc_fast2: FP32 evaluation of arc_cost for weight 1 and
- * coherences in [0, 1].  Each rounded decision is taken only when the FP32 value is farther from the
- * decision boundary than the bound on its distance to the reference's FP64
- * value, so the integers equal the reference's; otherwise returns false.
+ * coherences in [0, 1] (cor_fast).  Each rounded decision is taken only when
+ * the FP32 value is farther from the decision boundary than the bound on its
+ * distance to the reference's FP64 value, so the integers equal the
+ * reference's; otherwise the lane reports false.
  *  rho:    rho_f = RN(ca + cb)/2 is within 2^-23 relative of the reference's
  *          (ca + cb)/2, so rho_f >= thresh (1 + 2^-20) and rho_f <=
  *          thresh (1 - 2^-20) decide rho < thresh.
  *  offset: X = RN(RN(dp - sel) nsc) is within nsc 2^-23 of the reference's
- *          FP64 value; m_off = nsc 2^-22 + 2^-30 brackets half-integers
- *          (DEFO, rint) or integers (SMOOTH, trunc).
+ *          FP64 value, and |X| <= nsc <= 4096.  DEFO rounds to nearest: the
+ *          boundaries are the half-integers.  SMOOTH truncates: X - sign(X)/2
+ *          (exact for |X| >= 1/4, and rounding to 0 below) moves the
+ *          boundaries, the integers, to half-integers.  Either way XM =
+ *          RN(X' + 1.5 2^23) holds the nearest integer of X' in its low bits,
+ *          and |X' - (XM - 1.5 2^23)| <= 1/2 - m_off, m_off = nsc 2^-22 +
+ *          2^-30, keeps X' away from the boundaries.
  *  sigsq:  b = ((1 - ca) + (1 - cb))/2 is within 2^-22 relative of the
- *          reference's 1 - rho; for b >= 2^-8 the MUFU log2/exp2 estimate of
- *          b^rhopow and the FMA stay within 2e-6 rhopow + 5e-7 relative, and
- *          the screen (1e-5 (1 + rhopow) + 2e-6 relative + 1e-6) brackets the
- *          truncation point with at least a 5x margin.
+ *          reference's 1 - rho and b <= 1; for b >= 2^-8 the MUFU log2/exp2
+ *          estimate of b^rhopow and the FMA stay within 2e-6 rhopow + 5e-7
+ *          relative, so v = a b^rhopow + c is bracketed by the screen m =
+ *          (1e-5 (1 + rhopow) + 2e-6) v + 1e-6 with at least a 5x margin;
+ *          w = v - 1/2 rounded to the nearest integer gives floor(v), and
+ *          |w - round(w)| <= 1/2 - m keeps v that far from the integers.
+ *          v >= 0 and v < 1e6 hold for every b in [0, 1] (host-checked).
  *  rho = 0 uses the exact host value of the reference's formula at b = 1.
  * arc_lane takes one lane's decisions from the values arc_fast2 computed. */
 template <bool DEFO>
-__device__ __forceinline__ bool arc_lane(float ca, float cb, float rho, float X, float XM, float f,
-                                         float b, float v, float vm, float fr, float m,
-                                         const CostConsts &k, const short *lay, int ntab,
-                                         ArcCost &o)
+__device__ __forceinline__ bool arc_lane(bool pos, float rho, float XM, float f, float b, float vm,
+                                         float g, float mh, const CostConsts &k, const short *lay,
+                                         int ntab, ArcCost &o)
 {
-    bool ok = (ca >= 0.0f) & (ca <= 1.0f) & (cb >= 0.0f) & (cb <= 1.0f);
-    const bool pos = rho >= k.thr_hi;
-    ok &= pos | (rho <= k.thr_lo);
-    int off_i = __float_as_int(XM) - 0x4B400000;
+    bool ok = pos | (rho <= k.thr_lo);
+    ok &= fabsf(f) <= k.off_hm;
+    ok &= !pos | ((b >= 0x1p-8f) & (fabsf(g) <= mh));
+    int sg = pos ? __float_as_int(vm) - 0x4B400000 : k.s_rho0;
+    sg = max(sg, k.sigsqshortmin);
     if (DEFO) {
-        ok &= fabsf(f) <= 0.5f - k.m_off;
-    } else {
-        ok &= fabsf(f) >= k.m_off;
-        off_i += (f > 0.0f && X < 0.0f) ? 1 : 0;
-        off_i -= (f < 0.0f && X > 0.0f) ? 1 : 0;
-    }
-    const bool okp = (b >= 0x1p-8f) & (b <= 1.0f) & (v >= 0.0f) & (v < 1.0e6f) & (fr >= m) &
-                     (fr <= 1.0f - m);
-    ok &= !pos | okp;
-    const int sg = max(pos ? __float_as_int(vm) - 0x4B400000 : k.s_rho0, k.sigsqshortmin);
-    if (DEFO) {
-        ok &= sg < ntab;
+        /* the table holds every value of the fast path; the test only
+         * guards lanes that fail anyway */
+        ok &= (unsigned)sg < (unsigned)ntab;
         o.dzmax = (short)k.dzmax;
-        o.laycost = lay[min(max(sg, 0), ntab - 1)];
+        o.laycost = lay[min((unsigned)sg, (unsigned)(ntab - 1))];
     } else {
         o.dzmax = 0;
         o.laycost = 0;
+        sg = min(sg, (int)SHRT_MAX);
     }
-    off_i = min(max(off_i, (int)SHRT_MIN), (int)SHRT_MAX);
-    o.off = (short)off_i;
-    o.sigsq = (short)min(sg, (int)SHRT_MAX);
+    o.off = (short)(__float_as_int(XM) - 0x4B400000);
+    o.sigsq = (short)sg;
     return ok;
 }
 
-/* the two columns of a pair: the arithmetic on both lanes at
- * once (same roundings as the scalar forms), the decisions per lane.  Every
- * candidate is computed and each margin test folds into one predicate (a
- * NaN anywhere fails its test). */
+/* the two columns of a pair: the arithmetic on both lanes at once (same
+ * roundings as the scalar forms), the decisions per lane.  Every candidate
+ * is computed and each margin test folds into one predicate (a NaN anywhere
+ * fails its test). */
 template <bool DEFO>
 __device__ __forceinline__ void arc_fast2(float2 ca, float2 cb, float2 dp, float2 av,
                                           const CostConsts &k, const short *lay, int ntab,
@@ -577,22 +592,22 @@ __device__ __forceinline__ void arc_fast2(float2 ca, float2 cb, float2 dp, float
     const float2 half = f2(0.5f, 0.5f), one = f2(1.0f, 1.0f);
     const float2 mg = f2(12582912.0f, 12582912.0f);
     const float2 rho = __fmul2_rn(half, __fadd2_rn(ca, cb));
+    const bool pos0 = rho.x >= k.thr_hi, pos1 = rho.y >= k.thr_hi;
     const float2 hav = __fmul2_rn(half, av);
-    const float2 sel = f2(rho.x >= k.thr_hi ? av.x : hav.x, rho.y >= k.thr_hi ? av.y : hav.y);
-    const float2 X = __fmul2_rn(sub2(dp, sel), f2(k.nsc_f, k.nsc_f));
+    const float2 sel = f2(pos0 ? av.x : hav.x, pos1 ? av.y : hav.y);
+    float2 X = __fmul2_rn(sub2(dp, sel), f2(k.nsc_f, k.nsc_f));
+    if (!DEFO) X = sub2(X, f2(copysignf(0.5f, X.x), copysignf(0.5f, X.y)));
     const float2 XM = __fadd2_rn(X, mg);
     const float2 f = sub2(X, sub2(XM, mg));
-    /* sigsq for rho > 0 (FP32 screen); rho = 0 uses the exact host value */
     const float2 b = __fmul2_rn(half, __fadd2_rn(sub2(one, ca), sub2(one, cb)));
     const float2 t = __fmul2_rn(f2(k.rhopow_f, k.rhopow_f), f2(lg2_ftz(b.x), lg2_ftz(b.y)));
     const float2 v = __ffma2_rn(f2(k.a_f, k.a_f), f2(ex2_ftz(t.x), ex2_ftz(t.y)), f2(k.c_f, k.c_f));
-    const float2 vm = __fadd2_rn(sub2(v, half), mg);
-    const float2 fr = sub2(v, sub2(vm, mg));
-    const float2 m = __ffma2_rn(f2(k.screen_f, k.screen_f), v, f2(1e-6f, 1e-6f));
-    ok0 = arc_lane<DEFO>(ca.x, cb.x, rho.x, X.x, XM.x, f.x, b.x, v.x, vm.x, fr.x, m.x, k, lay,
-                         ntab, o0);
-    ok1 = arc_lane<DEFO>(ca.y, cb.y, rho.y, X.y, XM.y, f.y, b.y, v.y, vm.y, fr.y, m.y, k, lay,
-                         ntab, o1);
+    const float2 w = sub2(v, half);
+    const float2 vm = __fadd2_rn(w, mg);
+    const float2 g = sub2(w, sub2(vm, mg));
+    const float2 mh = __ffma2_rn(f2(-k.screen_f, -k.screen_f), v, f2(k.half_m, k.half_m));
+    ok0 = arc_lane<DEFO>(pos0, rho.x, XM.x, f.x, b.x, vm.x, g.x, mh.x, k, lay, ntab, o0);
+    ok1 = arc_lane<DEFO>(pos1, rho.y, XM.y, f.y, b.y, vm.y, g.y, mh.y, k, lay, ntab, o1);
 }
 
 template <bool DEFO>
@@ -758,6 +773,8 @@ __global__ void __launch_bounds__(256, MINB) k_costs7(const float *__restrict__ 
                 cv[h][q] = __ldg(corr + (size_t)rr * ncol + ac);
                 cw[h][q] = __ldg(corr + (size_t)rr * ncol + ac + 1);
             }
+            cv[h][q] = cor_fast(cv[h][q]);
+            if (q < 4) cw[h][q] = cor_fast(cw[h][q]);
         }
     }
 #pragma unroll
@@ -766,9 +783,8 @@ __global__ void __launch_bounds__(256, MINB) k_costs7(const float *__restrict__ 
         if (ar >= dr) break;
         const float2 avg = boxcar7(w + m);
         const float2 dps = S.dpp[(rs + m + 3) * kC7PP + j + 3];
-        const float2 ca2 = f2(sane(cv[0][m]), sane(cv[1][m]));
-        const float2 cb2 = FAM == 0 ? f2(sane(cv[0][m + 1]), sane(cv[1][m + 1]))
-                                    : f2(sane(cw[0][m]), sane(cw[1][m]));
+        const float2 ca2 = f2(cv[0][m], cv[1][m]);
+        const float2 cb2 = FAM == 0 ? f2(cv[0][m + 1], cv[1][m + 1]) : f2(cw[0][m], cw[1][m]);
         ArcCost of[2];
         bool okf[2] = {false, false};
         if (fast) arc_fast2<DEFO>(ca2, cb2, dps, avg, k, S.lay, ntab, of[0], of[1], okf[0], okf[1]);
@@ -777,7 +793,6 @@ __global__ void __launch_bounds__(256, MINB) k_costs7(const float *__restrict__ 
             const int ac = c0 + j + h * kC7H;
             if (ac >= dc) continue;
             const float dpv = h ? dps.y : dps.x, avv = h ? avg.y : avg.x;
-            const float ca = h ? ca2.y : ca2.x, cb = h ? cb2.y : cb2.x;
             const size_t a = FAM == 0 ? (size_t)ar * ncol + ac
                                       : nra + (size_t)ar * (ncol - 1) + ac;
             const short wt = weights ? weights[a] : (short)1;
@@ -789,6 +804,9 @@ __global__ void __launch_bounds__(256, MINB) k_costs7(const float *__restrict__ 
             } else if (wt == 1 && okf[h]) {
                 store_arc<DEFO>(costs_out, a, of[h]);
             } else {
+                /* the stored coherence (cor_fast changed values it rejects) */
+                const float *cp = corr + (size_t)ar * ncol + ac;
+                const float ca = sane(__ldg(cp)), cb = sane(__ldg(cp + (FAM == 0 ? ncol : 1)));
                 const int slot = atomicAdd(&S.qn, 1);
                 if (slot < kC7Q) {
                     S.q[slot] = C7Deferred{ca, cb, dpv, avv, (ar - r0) * kC7B + (ac - c0), (int)wt};

@@ -110,7 +110,8 @@ def test_costs_tiny_and_equal_phase_differences(torch_cuda):
 @pytest.mark.parametrize("nlooks", [1.0, 5.0, 20.0])
 def test_costs_at_decision_boundaries(torch_cuda, nlooks):
     """Coherence at the zero-coherence threshold (to a few ulps), near 1,
-    outside [0, 1], non-finite, and weights 0/1/2: the kernels' FP32 fast
+    outside [0, 1] (also just above 1 and -0), subnormal, non-finite, and
+    weights 0/1/2: the kernels' FP32 fast
     path must hand every arc it cannot decide to the exact arithmetic, so
     the costs equal the oracle's bit for bit."""
     rng = np.random.default_rng(int(nlooks))
@@ -127,6 +128,9 @@ def test_costs_at_decision_boundaries(torch_cuda, nlooks):
     g[90:110, :] = np.float32(1.0) - rng.integers(0, 400, size=(20, nc)).astype(np.float32) * 2.0 ** -24
     g[120:125, 30:90] = np.float32(1.25)
     g[126:128, 30:90] = np.float32(-0.5)
+    g[128, 30:90] = np.float32(-0.0)
+    g[129, 30:60] = np.nextafter(np.float32(1.0), np.float32(2.0))
+    g[129, 60:90] = np.float32(2.0 ** -149)
     g[130, 40:60] = np.nan
     g[131, 40:60] = np.inf
     narcs = (nr - 1) * nc + nr * (nc - 1)
