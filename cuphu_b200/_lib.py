@@ -150,6 +150,7 @@ SIGNATURES = {
     "cuphu_bridge_apply_test": (_I, [VP, VP, _I, _I, P(CuPhuBridgeParams), VP, _I]),
     "cuphu_bridge_device": (_I, [VP, VP, VP, _I, _I, P(CuPhuBridgeParams), VP]),
     "cuphu_test_skip_barrier_once": (_I, [_I, _I]),
+    "cuphu_test_force_solve_shape": (_I, [_I]),
     "cuphu_last_status": (_I, [_I]),
     "cuphu_release_workspace": (_I, [_I]),
 }

@@ -1,6 +1,7 @@
 """Launch-shape autotuner (cuphu_autotune): picks, per device and job size,
-the cost kernel's occupancy variant and the persistent solver's blocks per SM
-by timing both candidates on a representative scene."""
+the cost kernel's occupancy variant and the persistent solver's launch shape
+(stages of each block's shared-memory ring x resident blocks per SM) by
+timing the candidates on a representative scene."""
 from __future__ import annotations
 
 import ctypes as C
@@ -10,12 +11,15 @@ import numpy as np
 from ._lib import check, default_params, default_tile_params, lib, ptr
 
 _COST = {"smooth": 0, "defo": 1, "topo": 2}
+# the mixed-precision solver's launch shapes, in the library's index order
+_SOLVE_SHAPES = ((2, 3), (3, 2), (2, 2))
 
 
 def autotune(igram, corr, nlooks, cost="smooth", ntiles=(1, 1), tile_overlap=(0, 0), gpu_id=0):
     """Tune on this scene; the choices apply to later calls of similar size
     (same floor(log2) of the arc / work-item count) on this GPU.  Returns
-    {"cost_blocks_per_sm": 3 | 4, "solver_blocks_per_sm": 2 | 3}."""
+    {"cost_blocks_per_sm": 3 | 4, "solver_stages": S, "solver_blocks_per_sm": B}
+    for the mixed-precision solver's chosen shape."""
     ig = np.ascontiguousarray(igram, dtype=np.complex64)
     g = np.ascontiguousarray(corr, dtype=np.float32)
     nrow, ncol = g.shape
@@ -27,4 +31,6 @@ def autotune(igram, corr, nlooks, cost="smooth", ntiles=(1, 1), tile_overlap=(0,
     out = (C.c_int * 2)()
     check(lib().cuphu_autotune(ptr(ig.view(np.float32)), ptr(g), nrow, ncol, _COST[cost],
                                C.byref(p), C.byref(t), int(gpu_id), out))
-    return {"cost_blocks_per_sm": 3 + out[0], "solver_blocks_per_sm": out[1]}
+    stages, blocks = _SOLVE_SHAPES[out[1]]
+    return {"cost_blocks_per_sm": 3 + out[0], "solver_stages": stages,
+            "solver_blocks_per_sm": blocks}

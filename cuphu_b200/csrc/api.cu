@@ -1073,7 +1073,7 @@ int cuphu_autotune(const float *igram_c64, const float *corr, int nrow, int ncol
     if (!d_ig || !d_corr || !d_ph || !d_unw || !d_cost) rc = fail(CUPHU_ERR_ALLOC, "device allocation failed");
     Timers tm(rc ? 0 : 2);
     cudaEvent_t e0 = tm.e[0], e1 = tm.e[1];
-    int best_cost = 0, best_blocks = 3;
+    int best_cost = 0, best_shape = 0;
     if (!rc) {
         rc = copy_async(d_ig, igram_c64, 8 * n, cudaMemcpyHostToDevice, s, "H2D igram");
         if (!rc) rc = copy_async(d_corr, corr, 4 * n, cudaMemcpyHostToDevice, s, "H2D corr");
@@ -1098,13 +1098,16 @@ int cuphu_autotune(const float *igram_c64, const float *corr, int nrow, int ncol
     }
     tune_force(0, -1);
     if (!rc) tune_set(gpu_id, 0, 2LL * nrow * ncol, best_cost);
-    /* persistent solver: 2 or 3 blocks per SM, 20 PCG iterations, no IRLS */
+    /* persistent solver: each launch shape (ring stages x blocks per SM) of
+     * the default precision, 20 PCG iterations, no IRLS */
     best_ms = 1e30f;
     long long items = 0;
-    for (int per_sm = 2; per_sm <= 3 && !rc; ++per_sm) {
-        tune_force(1, per_sm);
-        CuPhuSolveOptions so;
-        default_solve_options(&so);
+    CuPhuSolveOptions so0;
+    default_solve_options(&so0);
+    const int nshape = solve_shape_count(so0.precision == CUPHU_PREC_FP64);
+    for (int v = 0; v < nshape && !rc; ++v) {
+        tune_force(1, v);
+        CuPhuSolveOptions so = so0;
         so.max_iter = 20;
         so.n_irls = 0;
         so.ref_row = so.ref_col = -1;
@@ -1113,15 +1116,15 @@ int cuphu_autotune(const float *igram_c64, const float *corr, int nrow, int ncol
             rc = cuphu_unwrap_device(nullptr, d_ph, d_corr, nullptr, nullptr, nrow, ncol, cost_mode,
                                      params, tile, &so, d_unw, nullptr, nullptr, &st, s);
         items = tune_probe_items();
-        if (!rc && st.solve_ms < best_ms) { best_ms = (float)st.solve_ms; best_blocks = per_sm; }
+        if (!rc && st.solve_ms < best_ms) { best_ms = (float)st.solve_ms; best_shape = v; }
     }
     tune_force(1, -1);
-    if (!rc && items > 0) tune_set(gpu_id, 1, items, best_blocks);
+    if (!rc && items > 0) tune_set(gpu_id, 1, items, best_shape);
     cudaError_t e = cudaStreamSynchronize(s);
     cudaFreeAsync(d_ig, s); cudaFreeAsync(d_corr, s); cudaFreeAsync(d_ph, s);
     cudaFreeAsync(d_unw, s); cudaFreeAsync(d_cost, s);
     if (!rc && e != cudaSuccess) rc = cuda_fail(e, "cuphu_autotune");
-    if (!rc && choices) { choices[0] = best_cost; choices[1] = best_blocks; }
+    if (!rc && choices) { choices[0] = best_cost; choices[1] = best_shape; }
     return rc;
 }
 
@@ -1294,7 +1297,15 @@ int cuphu_test_skip_barrier_once(int gpu_id, int block)
     return 0;
 }
 
-/* ── network-flow front-end inputs (the §8(f) GPU-side MCF inputs) ────── */
+int cuphu_test_force_solve_shape(int shape)
+{
+    if (shape < -1 || shape >= std::max(solve_shape_count(false), solve_shape_count(true)))
+        return fail(CUPHU_ERR_INVALID, "no such solver launch shape");
+    tune_force(1, shape);
+    return 0;
+}
+
+/* ── inputs of the CPU network-flow front end, computed on the GPU ─────── */
 int cuphu_mst_costs_device(const void *d_smooth_costs, long long narcs, long nshortcycle,
                            long maxcost, short *d_out, void *stream)
 {

@@ -134,6 +134,10 @@ int launch_solve(bool fp64, const TileDesc *tiles, const int *item_tile, int nit
                  int ntiles, const SolverPlanes &P, int plane_pitch, int plane_rows,
                  TileState *st, double *part, SolverCtl *ctl, const SolveParams &sp,
                  int device, cudaStream_t s);
+/* the solver's launch shapes (ring stages, blocks per SM) the autotuner
+ * chooses among, per precision; shape v of solve_shape_count(fp64) */
+int solve_shape_count(bool fp64);
+void solve_shape_of(bool fp64, int v, int *stages, int *blocks_per_sm);
 
 /* conncomp.cu */
 struct CcArgs {

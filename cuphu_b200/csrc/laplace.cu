@@ -266,10 +266,63 @@ __device__ __forceinline__ ItemXY item_xy(const TileDesc &T, int li)
     return q;
 }
 
+/* ── mixed-precision preconditioner and dots ─────────────────────────────
+ * diag32: the Jacobi diagonal as an FP32 sum of the positive in-tile arc
+ * weights (down, up, right, left) plus eps; rcp_pre: its reciprocal by the
+ * hardware approximation (rcp.approx, within 1 ulp).  M^-1 = rcp_pre(diag32)
+ * is the preconditioner of the mixed solve: every place that forms
+ * z = M^-1 r (the INIT/true-residual phase, an item's own pixels, its halo
+ * ring) evaluates these two functions on the same weights, so all blocks
+ * agree on M bit for bit and no division is needed. */
+__device__ __forceinline__ float diag32(int r, int c, int nr, int nc, float wdn, float wup,
+                                        float wrt, float wlf)
+{
+    float ws = 0.0f;
+    if (r < nr - 1 && wdn > 0.0f) ws = __fadd_rn(ws, wdn);
+    if (r > 0 && wup > 0.0f) ws = __fadd_rn(ws, wup);
+    if (c < nc - 1 && wrt > 0.0f) ws = __fadd_rn(ws, wrt);
+    if (c > 0 && wlf > 0.0f) ws = __fadd_rn(ws, wlf);
+    return __fadd_rn(ws, kLapEpsF);
+}
+
+__device__ __forceinline__ float rcp_pre(float d)
+{
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(d));
+    return y;
+}
+
+/* sum_j a[j] b[j] over a thread's four pixels with FP64 accuracy and no
+ * per-element conversion: each FP32 product is split exactly into
+ * p + e (e = fma(a, b, -p)), the p are summed with Knuth's TwoSum (the
+ * rounding error of each addition recovered exactly), and the small terms
+ * in FP32; hi + lo is then converted once.  For products in FP32's normal
+ * range the error is ~2^-44 of the sum of the magnitudes, far below what
+ * the FP64 tree reduction over a tile rounds away. */
+__device__ __forceinline__ double dot4_df(const float a[4], const float b[4])
+{
+    float hi = __fmul_rn(a[0], b[0]);
+    float lo = __fmaf_rn(a[0], b[0], -hi);
+#pragma unroll
+    for (int j = 1; j < 4; ++j) {
+        const float p = __fmul_rn(a[j], b[j]);
+        const float e = __fmaf_rn(a[j], b[j], -p);
+        const float s = __fadd_rn(hi, p);
+        const float bp = __fsub_rn(s, hi);
+        const float err = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bp)), __fsub_rn(p, bp));
+        hi = s;
+        lo = __fadd_rn(lo, __fadd_rn(e, err));
+    }
+    return (double)hi + (double)lo;
+}
+
 /* ── INIT / true residual: b, diag (A10) and r = b - A x, rz partial ────────
  * zero_x: first pass (x = 0, r = b).  write_diag: assemble pass (else the
- * stored diag is reused: residual replacement).  z = r / diag goes to zout
- * (mixed mode double-buffers z). */
+ * stored diag is reused: residual replacement).  FP64 mode: z = r / diag
+ * goes to zout.  Mixed mode: the FP32 residual r goes to zout (its
+ * double-buffered residual plane), the preconditioner is M^-1 =
+ * rcp_pre(diag32) recomputed from the weights, and the partial r.z comes
+ * from dot4_df. */
 template <typename V, bool WLS>
 __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, bool zero_x,
                              bool write_diag, V *zout)
@@ -290,8 +343,9 @@ __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, b
     size_t prow = (size_t)r * pitch;
     double xv[4];
     V rv[4], dv[4], zv[4];
+    float zf[4];   /* mixed: z = M^-1 r of the thread's pixels */
     if (!zero_x) ld4(x + prow + q.c0, xv);
-    if (!write_diag) ld4(dg + prow + q.c0, dv);
+    if (!write_diag && sizeof(V) == 8) ld4(dg + prow + q.c0, dv);
     double acc = 0.0;
 #pragma unroll
     for (int j = 0; j < kItemVx; ++j) {
@@ -299,6 +353,7 @@ __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, b
         if (c >= nc) {
             rv[j] = (V)0;
             zv[j] = (V)0;
+            zf[j] = 0.0f;
             if (write_diag) dv[j] = (V)0;
             if (zero_x) xv[j] = 0.0;
             continue;
@@ -306,12 +361,14 @@ __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, b
         size_t gi = (size_t)r * pp + c, pi = prow + c;
         float pa = gdp ? 0.0f : __ldg(ph + gi);
         double bv = 0.0, ws = 0.0;
+        float ws32 = 0.0f;   /* mixed: diag32's sum, in its order */
         if (r < nr - 1) {
             float w = ldc(wd + pi);
             if (w > 0.0f) {
                 float g = gdp ? ldc(gdp + pi) : lap_wrap_pi(__ldg(ph + gi + pp) - pa);
                 bv = __fma_rn(-(double)w, (double)g, bv);
                 ws += w;
+                ws32 = __fadd_rn(ws32, w);
             }
         }
         if (r > 0) {
@@ -320,6 +377,7 @@ __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, b
                 float g = gdp ? ldc(gdp + pi - pitch) : lap_wrap_pi(pa - __ldg(ph + gi - pp));
                 bv = __fma_rn((double)w, (double)g, bv);
                 ws += w;
+                ws32 = __fadd_rn(ws32, w);
             }
         }
         if (c < nc - 1) {
@@ -328,6 +386,7 @@ __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, b
                 float g = grp ? ldc(grp + pi) : lap_wrap_pi(__ldg(ph + gi + 1) - pa);
                 bv = __fma_rn(-(double)w, (double)g, bv);
                 ws += w;
+                ws32 = __fadd_rn(ws32, w);
             }
         }
         if (c > 0) {
@@ -336,6 +395,7 @@ __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, b
                 float g = grp ? ldc(grp + pi - 1) : lap_wrap_pi(pa - __ldg(ph + gi - 1));
                 bv = __fma_rn((double)w, (double)g, bv);
                 ws += w;
+                ws32 = __fadd_rn(ws32, w);
             }
         }
         if (rhsp) bv = (double)ldc(rhsp + pi);
@@ -353,13 +413,22 @@ __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, b
             if (c > 0)      y = __fma_rn((double)ldc(wr + pi - 1), xa - ldc(x + pi - 1), y);
         }
         V rs = (V)(bv - y);
-        V ds = (V)d;
-        double z = (double)rs / (double)ds;
-        acc = __fma_rn((double)rs, z, acc);
-        rv[j] = rs;
-        zv[j] = (V)z;
-        if (write_diag) dv[j] = ds;
+        if constexpr (sizeof(V) == 8) {
+            V ds = (V)d;
+            double z = (double)rs / (double)ds;
+            acc = __fma_rn((double)rs, z, acc);
+            rv[j] = rs;
+            zv[j] = (V)z;
+            if (write_diag) dv[j] = ds;
+        } else {
+            const float d32 = __fadd_rn(ws32, kLapEpsF);
+            rv[j] = rs;
+            zf[j] = __fmul_rn((float)rs, rcp_pre(d32));
+            zv[j] = rs;
+            if (write_diag) dv[j] = (V)d32;
+        }
     }
+    if constexpr (sizeof(V) == 4) acc = dot4_df((const float *)rv, zf);
     if (sizeof(V) == 8) st4(rr + prow + q.c0, rv);
     st4(zout + T.pix + prow + q.c0, zv);
     if (write_diag) st4(dg + prow + q.c0, dv);
@@ -430,7 +499,6 @@ struct StageS {
     static constexpr uint32_t kTxWd = (uint32_t)(kWdH * kSegW * 4);
     static constexpr uint32_t kTxDx = (uint32_t)(kItemBy * kItemBx * 4);
 };
-constexpr int kStages = 2;
 template <typename V> __host__ __device__ constexpr size_t stage_bytes()
 {
     return sizeof(V) == 4 ? StageS::kBytes
@@ -443,9 +511,10 @@ template <typename V> __host__ __device__ constexpr size_t pn_bytes()
 {
     return al128((size_t)kHaloH * kSegW * sizeof(V));
 }
-template <typename V> __host__ __device__ constexpr size_t solve_smem_bytes()
+/* NS: stages of the shared-memory ring (items in flight per block) */
+template <typename V, int NS> __host__ __device__ constexpr size_t solve_smem_bytes()
 {
-    return kStages * stage_bytes<V>() + pn_bytes<V>() + 128;
+    return NS * stage_bytes<V>() + pn_bytes<V>() + 128;
 }
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p)
@@ -707,28 +776,19 @@ __device__ __forceinline__ void issue_s(const TileDesc &T, int li, const SolveMa
 /* Jacobi diagonal of pixel (r, c) from its four arc weights, in the
  * assembly's order and arithmetic (phase_init): an FP64 sum of the positive
  * weights of the arcs inside the tile, plus eps, rounded to float */
-__device__ __forceinline__ float diag_of(int r, int c, int nr, int nc, float wdn, float wup,
-                                         float wrt, float wlf)
-{
-    double ws = 0.0;
-    if (r < nr - 1 && wdn > 0.0f) ws += wdn;
-    if (r > 0 && wup > 0.0f) ws += wup;
-    if (c < nc - 1 && wrt > 0.0f) ws += wrt;
-    if (c > 0 && wlf > 0.0f) ws += wlf;
-    return (float)(ws + (double)kLapEpsF);
-}
-
 /* One item of the mixed pass.  FP32 arithmetic for the vector updates and
- * the stencil (IEEE round-to-nearest per operation), FP64 accumulation of
- * the four dots: acc[0] r.z of the updated residual (when not fresh),
- * acc[1] p.q, acc[2] z.q, acc[3] q.(q/diag). */
+ * the stencil (IEEE round-to-nearest per operation), FP64-accurate dots
+ * (dot4_df per thread, FP64 tree across the item): acc[0] r.z of the
+ * updated residual (when not fresh), acc[1] p.q, acc[2] z.q, acc[3]
+ * q.(M^-1 q).  The residual plane holds r; z = M^-1 r is formed on the fly
+ * with M^-1 = rcp_pre(diag32) of the staged weights. */
 __device__ __forceinline__ void compute_s(const TileDesc &T, int li, float *pnew_all,
-                                          float *znew_all, float *qnew_all, float *dx_all,
+                                          float *rnew_all, float *qnew_all, float *dx_all,
                                           bool first, bool fresh, float alphaf, float betaf,
                                           const char *stage, float *Pn, double acc[kNComp])
 {
     const int r0b = (li / T.nbx) * kItemBy, c0b = (li % T.nbx) * kItemBx;
-    const float *Z = (const float *)(stage + StageS::oZ);
+    const float *R = (const float *)(stage + StageS::oZ);
     const float *Q = (const float *)(stage + StageS::oQ);
     const float *PO = (const float *)(stage + StageS::oPO);
     const float *WR = (const float *)(stage + StageS::oWR);
@@ -743,9 +803,9 @@ __device__ __forceinline__ void compute_s(const TileDesc &T, int li, float *pnew
      * column jc <-> c0b - 4 + jc */
     const int so = (ty + 1) * kSegW + 4 + tx * kItemVx;
     const int sd = so + kSegW;                 /* wd(r, c) in the down-arc box */
-    /* only z' and diag of the own pixels stay in registers across the
+    /* only z' and M^-1 of the own pixels stay in registers across the
      * barrier; p' and the weights are read back from shared memory */
-    float zn[4] = {0.f, 0.f, 0.f, 0.f}, dg[4] = {1.f, 1.f, 1.f, 1.f};
+    float zn[4] = {0.f, 0.f, 0.f, 0.f}, rd[4] = {0.f, 0.f, 0.f, 0.f};
     const size_t o = T.pix + (size_t)r * T.pitch + c0;
     {
         float pn[4] = {0.f, 0.f, 0.f, 0.f};
@@ -755,9 +815,9 @@ __device__ __forceinline__ void compute_s(const TileDesc &T, int li, float *pnew
             sld4(WD + sd - kSegW, wup);
             sld4(WR + so, wrt);
             const float wlf = WR[so - 1];
-            float zv[4], qv[4] = {0.f, 0.f, 0.f, 0.f}, pv[4] = {0.f, 0.f, 0.f, 0.f};
+            float rv[4], qv[4] = {0.f, 0.f, 0.f, 0.f}, pv[4] = {0.f, 0.f, 0.f, 0.f};
             float dxv[4] = {0.f, 0.f, 0.f, 0.f};
-            sld4(Z + so, zv);
+            sld4(R + so, rv);
             if (!fresh) {
                 sld4(Q + so, qv);
                 sld4(DX + ty * kItemBx + tx * kItemVx, dxv);
@@ -766,22 +826,23 @@ __device__ __forceinline__ void compute_s(const TileDesc &T, int li, float *pnew
 #pragma unroll
             for (int j = 0; j < kItemVx; ++j) {
                 const int c = c0 + j;
-                if (c >= nc) continue;
-                const float d = diag_of(r, c, nr, nc, wdn[j], wup[j], wrt[j], j == 0 ? wlf : wrt[j - 1]);
-                float z = zv[j];
+                if (c >= nc) {
+                    rv[j] = 0.f;
+                    continue;
+                }
+                rd[j] = rcp_pre(diag32(r, c, nr, nc, wdn[j], wup[j], wrt[j],
+                                       j == 0 ? wlf : wrt[j - 1]));
                 if (!fresh) {
-                    const float rn = __fmaf_rn(-alphaf, qv[j], __fmul_rn(z, d));
-                    z = __fdiv_rn(rn, d);
-                    acc[0] = __fma_rn((double)rn, (double)z, acc[0]);
+                    rv[j] = __fmaf_rn(-alphaf, qv[j], rv[j]);
                     dxv[j] = __fmaf_rn(alphaf, pv[j], dxv[j]);
                 }
-                zn[j] = z;
-                dg[j] = d;
-                pn[j] = first ? z : __fmaf_rn(betaf, pv[j], z);
+                zn[j] = __fmul_rn(rv[j], rd[j]);
+                pn[j] = first ? zn[j] : __fmaf_rn(betaf, pv[j], zn[j]);
             }
             if (!fresh) {
+                acc[0] = dot4_df(rv, zn);
                 st4(dx_all + o, dxv);
-                st4(znew_all + o, zn);
+                st4(rnew_all + o, rv);
             }
         }
 #pragma unroll
@@ -798,12 +859,10 @@ __device__ __forceinline__ void compute_s(const TileDesc &T, int li, float *pnew
         float v = 0.f;
         if (gr >= 0 && gr < nr && gc >= 0 && gc < nc) {
             const int sidx = i * kSegW + jc;
-            float z = Z[sidx];
-            if (!fresh) {
-                const float d = diag_of(gr, gc, nr, nc, WD[sidx + kSegW], WD[sidx], WR[sidx],
-                                        WR[sidx - 1]);
-                z = __fdiv_rn(__fmaf_rn(-alphaf, Q[sidx], __fmul_rn(z, d)), d);
-            }
+            const float m = rcp_pre(diag32(gr, gc, nr, nc, WD[sidx + kSegW], WD[sidx], WR[sidx],
+                                           WR[sidx - 1]));
+            const float rr = fresh ? R[sidx] : __fmaf_rn(-alphaf, Q[sidx], R[sidx]);
+            const float z = __fmul_rn(rr, m);
             v = first ? z : __fmaf_rn(betaf, PO[sidx], z);
         }
         Pn[i * kSegW + jc] = v;
@@ -819,10 +878,14 @@ __device__ __forceinline__ void compute_s(const TileDesc &T, int li, float *pnew
         sld4(WD + sd - kSegW, wup);
         sld4(WR + so, wrt);
         const float wlf = WR[so - 1];
+        float mq[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
         for (int j = 0; j < kItemVx; ++j) {
             const int c = c0 + j;
-            if (c >= nc) continue;
+            if (c >= nc) {
+                pn[j] = 0.f;
+                continue;
+            }
             const float xl = j == 0 ? lf : pn[j - 1];
             const float xr = j == kItemVx - 1 ? rt : pn[j + 1];
             const float wl = j == 0 ? wlf : wrt[j - 1];
@@ -833,10 +896,11 @@ __device__ __forceinline__ void compute_s(const TileDesc &T, int li, float *pnew
             if (c < nc - 1) y = __fmaf_rn(wrt[j], __fsub_rn(xa, xr), y);
             if (c > 0)      y = __fmaf_rn(wl, __fsub_rn(xa, xl), y);
             qv[j] = y;
-            acc[1] = __fma_rn((double)xa, (double)y, acc[1]);
-            acc[2] = __fma_rn((double)zn[j], (double)y, acc[2]);
-            acc[3] = __fma_rn((double)y, (double)__fdiv_rn(y, dg[j]), acc[3]);
+            mq[j] = __fmul_rn(y, rd[j]);
         }
+        acc[1] = dot4_df(pn, qv);
+        acc[2] = dot4_df(zn, qv);
+        acc[3] = dot4_df(qv, mq);
         st4(pnew_all + o, pn);
         st4(qnew_all + o, qv);
     }
@@ -1103,18 +1167,17 @@ __device__ __forceinline__ Cursor cursor_active(Cursor c, const SliceCtl &sc, co
 }
 
 /* run a staged FP64 pass over this block's slice.  KIND 0: the stencil
- * pass, KIND 1: the update pass.  kStages items are in flight; the stage of
- * item k is refilled with item k+kStages right after the barrier of item k's
+ * pass, KIND 1: the update pass.  NS items are in flight; the stage of
+ * item k is refilled with item k+NS right after the barrier of item k's
  * reduction, which every thread reaches only after its last read of the
  * stage and Pn. */
-template <int KIND>
+template <int KIND, int NS>
 __device__ void run_pass(const SliceCtl &sc, const TileDesc *gt, const TileState *st, int ntiles,
                          const SolverPlanes &P, const SolveMaps &M, int psel, double *pvec,
                          bool flag, double *part, double *tot, unsigned *cnt, double *sw,
                          double *s_bcast, int *s_flag, double *Pn, char *stages, uint64_t *bars,
                          uint32_t &parity, SolverCtl *ctl, long long timeout_ns)
 {
-    constexpr int NS = kStages;
     constexpr size_t SB = stage_bytes<double>();
     const bool red = KIND == 0 || flag;
     if (sc.s0 >= sc.s1) return;
@@ -1172,6 +1235,7 @@ __device__ void run_pass(const SliceCtl &sc, const TileDesc *gt, const TileState
 
 /* the mixed single-synchronisation pass over this block's slice, staged
  * like run_pass, with kNComp partials per item */
+template <int NS>
 __device__ void run_pass_s(const SliceCtl &sc, const TileDesc *gt, const TileState *st, int ntiles,
                            int nitems, const SolveMaps &M, int zsel, int ksel, bool first,
                            bool fresh, float *pnew, float *znew, float *qnew, float *dx,
@@ -1180,7 +1244,6 @@ __device__ void run_pass_s(const SliceCtl &sc, const TileDesc *gt, const TileSta
                            char *stages, uint64_t *bars, uint32_t &parity, SolverCtl *ctl,
                            long long timeout_ns)
 {
-    constexpr int NS = kStages;
     constexpr size_t SB = stage_bytes<float>();
     if (sc.s0 >= sc.s1) return;
     Cursor ci = cursor_active(Cursor{sc.s0, sc.t0}, sc, gt, st, ntiles);
@@ -1243,9 +1306,6 @@ __device__ __forceinline__ TileState load_state(const TileState *p)
     return S;
 }
 
-#ifndef CUPHU_SOLVE_MIN_BLOCKS
-#define CUPHU_SOLVE_MIN_BLOCKS 3
-#endif
 
 /* A tile leaves the solve: the owner block updates the active count and the
  * statistics (pixel-iterations, the pass's largest iteration count). */
@@ -1298,8 +1358,8 @@ __device__ __forceinline__ void carry_inactive(const TileState *from, TileState 
 /* WLS = true: the WLS-mode instance (explicit arc targets / right-hand
  * side, optional warm start, no anchoring); a separate instantiation so the
  * main path's register allocation does not carry its extra inputs */
-template <typename V, bool WLS>
-__global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
+template <typename V, bool WLS, int NS, int MINB>
+__global__ void __launch_bounds__(kItemThreads, MINB)
     k_solve(const TileDesc *__restrict__ tiles, const int *__restrict__ item_tile, int nitems,
             int ntiles, SolverPlanes P, TileState *st, double *part, SolverCtl *ctl,
             SolveParams sp, long long timeout_ns, const __grid_constant__ SolveMaps M)
@@ -1309,7 +1369,7 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
     __shared__ double sw4[2][kNComp][8];
     __shared__ double s_bcast;
     __shared__ int s_flag;
-    __shared__ __align__(8) uint64_t bars[kStages];
+    __shared__ __align__(8) uint64_t bars[NS];
     __shared__ SliceCtl sc;
     char *dsm = (char *)(((uintptr_t)dsm_raw + 127) & ~(uintptr_t)127);
     constexpr bool mixed = sizeof(V) == 4;
@@ -1322,14 +1382,14 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
                        part + 2 * (size_t)kNComp * nitems + (size_t)kNComp * ntiles};
     unsigned *tick = reinterpret_cast<unsigned *>(part + 2 * (size_t)kNComp * nitems +
                                                   2 * (size_t)kNComp * ntiles);
-    V *Pn = (V *)(dsm + kStages * stage_bytes<V>());
+    V *Pn = (V *)(dsm + NS * stage_bytes<V>());
     /* z buffers: the first is written by the assembly; mixed mode
      * double-buffers z in the r plane (r = z diag is not stored) */
     V *zb[2] = {(V *)P.z, (V *)P.r};
     uint32_t parity = 0u;
     (void)item_tile;
     if (threadIdx.x == 0) {
-        for (int k = 0; k < kStages; ++k) mbar_init(&bars[k]);
+        for (int k = 0; k < NS; ++k) mbar_init(&bars[k]);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -1387,7 +1447,7 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
                     put_state(sc, stA, t, S, owner);
                 }
                 __syncthreads();
-                run_pass<0>(sc, tiles, stA, ntiles, P, M, it & 1, pnew, it == 0, pbuf[pc & 1],
+                run_pass<0, NS>(sc, tiles, stA, ntiles, P, M, it & 1, pnew, it == 0, pbuf[pc & 1],
                             tbuf[pc & 1], tick, sw, &s_bcast, &s_flag, (double *)Pn, dsm, bars,
                             parity, ctl, timeout_ns);
                 ++pc;
@@ -1413,7 +1473,7 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
                     put_state(sc, stB, t, S, owner);
                 }
                 __syncthreads();
-                run_pass<1>(sc, tiles, stB, ntiles, P, M, (it + 1) & 1, pnew, true, pbuf[pc & 1],
+                run_pass<1, NS>(sc, tiles, stB, ntiles, P, M, (it + 1) & 1, pnew, true, pbuf[pc & 1],
                             tbuf[pc & 1], tick, sw, &s_bcast, &s_flag, (double *)Pn, dsm, bars,
                             parity, ctl, timeout_ns);
                 ++pc;
@@ -1527,7 +1587,7 @@ __global__ void __launch_bounds__(kItemThreads, CUPHU_SOLVE_MIN_BLOCKS)
                     cur ^= 1;
                     fresh = true;
                 }
-                run_pass_s(sc, tiles, st + (size_t)cur * ntiles, ntiles, nitems, M, zsel, k & 1,
+                run_pass_s<NS>(sc, tiles, st + (size_t)cur * ntiles, ntiles, nitems, M, zsel, k & 1,
                            k == 0, fresh, (float *)pb[(k + 1) & 1], (float *)zb[zsel ^ 1],
                            qb[(k + 1) & 1], P.dx, pbuf[pc & 1], tbuf[pc & 1], tick, sw, sw4,
                            &s_bcast, &s_flag, (float *)Pn, dsm, bars, parity, ctl, timeout_ns);
@@ -1639,30 +1699,33 @@ static int make_maps(SolveMaps &M, const SolverPlanes &P, int pitch, int rows)
     return rc ? CUPHU_ERR_CUDA : 0;
 }
 
-template <typename V, bool WLS>
-static int launch_solve_kernel(const TileDesc *tiles, const int *item_tile, int nitems, int ntiles,
-                          const SolverPlanes &P, int pitch, int rows, TileState *st, double *part,
-                          SolverCtl *ctl, const SolveParams &sp, long long timeout_ns, int device,
-                          cudaStream_t s)
+/* Launch shapes of the persistent solver: the stages of each block's
+ * shared-memory ring (items whose boxes are in flight) and the resident
+ * blocks per SM it is compiled for (the launch bound, which sets the
+ * registers a thread may use).  Deeper rings keep more bytes in flight per
+ * SM; more blocks hide more latency.  The arithmetic and its order do not
+ * depend on the shape, so every shape gives identical results; the
+ * autotuner times them and keeps the fastest per job size. */
+template <typename V, bool WLS, int NS, int MINB>
+static int launch_solve_shape(const TileDesc *tiles, const int *item_tile, int nitems,
+                              int ntiles, const SolverPlanes &P, int pitch, int rows,
+                              TileState *st, double *part, SolverCtl *ctl, const SolveParams &sp,
+                              long long timeout_ns, int device, cudaStream_t s)
 {
-    if (ntiles > kMaxTiles)
-        return fail(CUPHU_ERR_INVALID, "at most 1024 tiles per solver launch");
     SolveMaps M;
     std::memset(&M, 0, sizeof(M));
     int rcm = make_maps<V>(M, P, pitch, rows);
     if (rcm) return rcm;
     int nsm = 0, per_sm = 0;
     CUPHU_TRY_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
-    const size_t smem = solve_smem_bytes<V>();
-    CUPHU_TRY_CUDA(cudaFuncSetAttribute(k_solve<V, WLS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    const size_t smem = solve_smem_bytes<V, NS>();
+    auto kern = k_solve<V, WLS, NS, MINB>;
+    CUPHU_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)smem));
-    CUPHU_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve<V, WLS>,
-                                                                 kItemThreads, smem));
+    CUPHU_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kItemThreads,
+                                                                 smem));
     if (per_sm < 1) return fail(CUPHU_ERR_CUDA, "solver kernel cannot be resident");
-    /* blocks per SM from the autotuner (job size = item count) */
-    tune_note_items(nitems);
-    const int tuned = tune_get(device, 1, (long long)nitems);
-    if (tuned >= 1) per_sm = std::min(per_sm, tuned);
+    per_sm = std::min(per_sm, MINB);
     int grid = std::min(nsm * per_sm, std::max(nitems, 1));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
@@ -1674,9 +1737,51 @@ static int launch_solve_kernel(const TileDesc *tiles, const int *item_tile, int 
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    CUPHU_TRY_CUDA(cudaLaunchKernelEx(&cfg, k_solve<V, WLS>, tiles, item_tile, nitems, ntiles, P, st,
-                                      part, ctl, sp, timeout_ns, M));
+    CUPHU_TRY_CUDA(cudaLaunchKernelEx(&cfg, kern, tiles, item_tile, nitems, ntiles, P, st, part,
+                                      ctl, sp, timeout_ns, M));
     return 0;
+}
+
+template <typename V, bool WLS>
+static int launch_solve_kernel(const TileDesc *tiles, const int *item_tile, int nitems, int ntiles,
+                          const SolverPlanes &P, int pitch, int rows, TileState *st, double *part,
+                          SolverCtl *ctl, const SolveParams &sp, long long timeout_ns, int device,
+                          cudaStream_t s)
+{
+    if (ntiles > kMaxTiles)
+        return fail(CUPHU_ERR_INVALID, "at most 1024 tiles per solver launch");
+    /* the shape from the autotuner (job size = item count) */
+    tune_note_items(nitems);
+    const int v = tune_get(device, 1, (long long)nitems);
+#define CUPHU_SOLVE_SHAPE(NS, MINB)                                                            \
+    return launch_solve_shape<V, WLS, NS, MINB>(tiles, item_tile, nitems, ntiles, P, pitch,    \
+                                                rows, st, part, ctl, sp, timeout_ns, device, s)
+    if constexpr (sizeof(V) == 4) {
+        switch (v) {
+        case 1: CUPHU_SOLVE_SHAPE(3, 2);
+        case 2: CUPHU_SOLVE_SHAPE(2, 2);
+        default: CUPHU_SOLVE_SHAPE(2, 3);
+        }
+    } else {
+        switch (v) {
+        case 1: CUPHU_SOLVE_SHAPE(3, 1);
+        default: CUPHU_SOLVE_SHAPE(2, 2);
+        }
+    }
+#undef CUPHU_SOLVE_SHAPE
+}
+
+int solve_shape_count(bool fp64) { return fp64 ? 2 : 3; }
+
+void solve_shape_of(bool fp64, int v, int *stages, int *blocks_per_sm)
+{
+    static const int mixed[3][2] = {{2, 3}, {3, 2}, {2, 2}};
+    static const int f64[2][2] = {{2, 2}, {3, 1}};
+    const int(*t)[2] = fp64 ? f64 : mixed;
+    const int n = solve_shape_count(fp64);
+    if (v < 0 || v >= n) v = 0;
+    *stages = t[v][0];
+    *blocks_per_sm = t[v][1];
 }
 
 template <typename V>

@@ -268,14 +268,15 @@ int cuphu_laplace_solve_device(const void *d_costs, int cost_stride_shorts,
 
 /* ── launch-shape autotuner (new) ─────────────────────────────────────────
  * Times, on the caller's scene (host pointers, uploaded here), the cost
- * kernel at 3 and 4 blocks per SM and the persistent solver at 2 and 3
- * blocks per SM (a 20-iteration probe with the given tiling), and stores the
- * faster choice per device and job-size class (floor(log2) of the arc or
- * work-item count) for all later calls.  choices (optional, int[2]) receives
- * {cost variant 0|1, solver blocks per SM}.  Costs and FP64 solves are
- * identical for every choice; mixed-precision update passes reduce in the
- * grid's segmentation, so a mixed solve is deterministic per choice.
- * CUPHU_TUNE=0 in the environment ignores stored choices. */
+ * kernel at 3 and 4 blocks per SM and the persistent solver in each of its
+ * launch shapes (stages of the per-block shared-memory ring x resident
+ * blocks per SM; mixed precision: 2x3, 3x2, 2x2) with a 20-iteration probe
+ * of the given tiling, and stores the fastest choice per device and
+ * job-size class (floor(log2) of the arc or work-item count) for all later
+ * calls.  choices (optional, int[2]) receives {cost variant 0|1, solver
+ * shape index}.  Results are identical for every choice: the per-item and
+ * per-tile reductions do not depend on the launch shape.  CUPHU_TUNE=0 in
+ * the environment ignores stored choices. */
 int cuphu_autotune(const float *igram_c64, const float *corr, int nrow, int ncol,
                    CuPhuCostMode cost_mode, const CuPhuParams *params,
                    const CuPhuTileParams *tile, int gpu_id, int *choices);
@@ -448,6 +449,12 @@ int cuphu_gpu_info(int device, long long *total_memory, int *sm_count, int *cc_m
  * device status becomes CUPHU_ERR_TIMEOUT (read by cuphu_last_status, or
  * returned by calls that wait).  One-shot: later launches are normal. */
 int cuphu_test_skip_barrier_once(int gpu_id, int block);
+
+/* test hook (new): solves launched later from the calling thread use launch
+ * shape `shape` of the persistent solver (the index of cuphu_autotune's
+ * choices[1]; an index beyond the precision's shapes selects shape 0),
+ * overriding stored autotuner choices; -1 restores the normal choice. */
+int cuphu_test_force_solve_shape(int shape);
 
 /* wait for the last pipeline enqueued on a device and return its device-side
  * status (CUPHU_ERR_TIMEOUT when a grid barrier gave up) (new) */

@@ -26,19 +26,21 @@ def test_mcf_inputs_smooth(torch_cuda, shape, nlooks):
     ig, g, _, _ = S.bumps(*shape, seed=shape[0], nbumps=3, amp_range=(10, 30),
                           sigma_range=(10, 30), nlooks=nlooks)
     g = g.copy()
-    g[10:30, 5:60] = 0.02                       # masked-out arcs: sigsq = LARGESHORT
+    g[10:30, 5:60] = 0.02                       # low coherence
     ig = np.ascontiguousarray(ig, np.complex64)
     nr, nc = g.shape
     narcs = (nr - 1) * nc + nr * (nc - 1)
+    w = np.ones(narcs, np.int16)
+    w[1000:1400] = 0                            # masked-out arcs: sigsq = LARGESHORT
     p = default_params(nlooks=nlooks, ncorrlooks=nlooks)
     costs = np.empty((narcs, 2), np.int16)
     mst = np.empty(narcs, np.int16)
     res = np.empty((nr - 1, nc - 1), np.int8)
     re, im = np.ascontiguousarray(ig.real), np.ascontiguousarray(ig.imag)
-    check(lib().cuphu_mcf_inputs(ptr(re), ptr(im), ptr(g), None, nr, nc, 0, C.byref(p), 0,
+    check(lib().cuphu_mcf_inputs(ptr(re), ptr(im), ptr(g), ptr(w), nr, nc, 0, C.byref(p), 0,
                                  ptr(costs), ptr(mst), ptr(res)))
     ph = O.phase_from_igram(ig)
-    want = O.build_costs(ph, g, nlooks, mode=0)
+    want = O.build_costs(ph, g, nlooks, mode=0, weights=w)
     assert np.array_equal(costs, want)
     assert np.array_equal(res, O.residues(ph))
     pos, neg, _ = O.incrcost(want, np.zeros(narcs, np.int16), nshortcycle=200, nflow=1)

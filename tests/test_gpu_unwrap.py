@@ -149,12 +149,33 @@ def test_autotune_keeps_results(torch_cuda):
                                       n_irls=2)
     ch = cuphu_b200.autotune(ig, g, 5.0, cost="defo", ntiles=(2, 2), tile_overlap=(16, 16))
     assert ch["cost_blocks_per_sm"] in (3, 4) and ch["solver_blocks_per_sm"] in (2, 3)
+    assert ch["solver_stages"] in (2, 3)
     u, c, _ = device_unwrap(torch_cuda, ph, g, 5.0, (2, 2), (16, 16), precision=1, n_irls=2)
     assert np.array_equal(u.view(np.int32), base_u.view(np.int32))
     assert np.array_equal(c, base_c)
     from tests.test_gpu_kernels import gpu_costs
     got = gpu_costs(torch_cuda, ph, g, 5.0, 1)
     assert np.array_equal(got, O.build_costs(ph, g, 5.0, mode=1))
+
+
+def test_solver_launch_shapes_give_identical_results(torch_cuda):
+    """Every launch shape of the persistent solver (ring stages x resident
+    blocks per SM) gives bit-identical unwraps and labels, in both
+    precisions: the reductions do not depend on the shape."""
+    ig, g, _, _ = S.bumps(230, 300, seed=62, nbumps=3, amp_range=(5, 25), sigma_range=(8, 30))
+    ph = O.phase_from_igram(ig)
+    for prec, nshape in ((0, 3), (1, 2)):
+        outs = []
+        for v in range(nshape):
+            check(lib().cuphu_test_force_solve_shape(v))
+            try:
+                outs.append(device_unwrap(torch_cuda, ph, g, 5.0, (2, 2), (16, 16),
+                                          precision=prec, n_irls=2)[:2])
+            finally:
+                check(lib().cuphu_test_force_solve_shape(-1))
+        for u, c in outs[1:]:
+            assert np.array_equal(u.view(np.int32), outs[0][0].view(np.int32))
+            assert np.array_equal(c, outs[0][1])
 
 
 def test_reference_pixel_shift_and_cc_on_device(torch_cuda):
