@@ -156,31 +156,6 @@ __device__ void seg_done(const TileDesc &T, int t, int nseg, const double *part,
     }
 }
 
-/* The kNComp block trees of one item in one barrier (the mixed pass reduces
- * four dots per item): per component the same shuffle-down tree per warp
- * and warp-0 tree as block_sum_item, results in thread 0.  `half` selects
- * one of the two scratch halves, as consecutive items alternate. */
-__device__ __forceinline__ void block_sum4_item(double v[kNComp], double (*sw4)[kNComp][8],
-                                                int half)
-{
-#pragma unroll
-    for (int c = 0; c < kNComp; ++c)
-        for (int off = 16; off > 0; off >>= 1) v[c] += __shfl_down_sync(0xffffffffu, v[c], off);
-    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    if (lane == 0)
-#pragma unroll
-        for (int c = 0; c < kNComp; ++c) sw4[half][c][w] = v[c];
-    __syncthreads();
-    if (w == 0) {
-#pragma unroll
-        for (int c = 0; c < kNComp; ++c) {
-            double x = lane < (int)(blockDim.x >> 5) ? sw4[half][c][lane] : 0.0;
-            for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
-            v[c] = x;
-        }
-    }
-}
-
 /* seg_done for the kNComp-component partials of the mixed pass: component c
  * of item i at part[c * nitems + i], of tile t at tot[c * ntiles + t] */
 __device__ void seg_done4(const TileDesc &T, int t, int nseg, const double *part, int nitems,
@@ -328,7 +303,8 @@ __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, b
                              bool write_diag, V *zout)
 {
     ItemXY q = item_xy(T, li);
-    if (q.r >= T.nr || q.c0 >= T.nc) return 0.0;
+    /* the mixed kernel's producer warp owns no pixels */
+    if (threadIdx.x >= kItemThreads || q.r >= T.nr || q.c0 >= T.nc) return 0.0;
     double *x = P.x + T.pix;
     V *rr = (V *)P.r + T.pix;
     V *dg = (V *)P.diag + T.pix;
@@ -514,7 +490,21 @@ template <typename V> __host__ __device__ constexpr size_t pn_bytes()
 /* NS: stages of the shared-memory ring (items in flight per block) */
 template <typename V, int NS> __host__ __device__ constexpr size_t solve_smem_bytes()
 {
-    return NS * stage_bytes<V>() + pn_bytes<V>() + 128;
+    /* mixed mode double-buffers Pn by item parity */
+    return NS * stage_bytes<V>() + (sizeof(V) == 4 ? 2 : 1) * pn_bytes<V>() + 128;
+}
+/* threads per block: mixed mode adds the producer warp */
+template <typename V> __host__ __device__ constexpr int solve_threads()
+{
+    return sizeof(V) == 4 ? kItemThreads + 32 : kItemThreads;
+}
+/* registers per thread that let MINB blocks be resident on one SM (65536
+ * registers, allocated per thread in multiples of 8), at most 255 */
+template <typename V, int MINB> __host__ __device__ constexpr int solve_regs()
+{
+    return (65536 / (MINB * solve_threads<V>())) / 8 * 8 > 255
+               ? 255
+               : (65536 / (MINB * solve_threads<V>())) / 8 * 8;
 }
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p)
@@ -524,6 +514,16 @@ __device__ __forceinline__ uint32_t smem_addr(const void *p)
 __device__ __forceinline__ void mbar_init(uint64_t *bar)
 {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+}
+/* an mbarrier that completes a phase after `count` plain arrivals */
+__device__ __forceinline__ void mbar_init_n(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 __device__ __forceinline__ void mbar_expect(uint64_t *bar, uint32_t bytes)
 {
@@ -773,81 +773,93 @@ __device__ __forceinline__ void issue_s(const TileDesc &T, int li, const SolveMa
     if (!fresh) tma_load_2d(stage + StageS::oDX, &M.xB, c0b, y, bar);
 }
 
-/* Jacobi diagonal of pixel (r, c) from its four arc weights, in the
- * assembly's order and arithmetic (phase_init): an FP64 sum of the positive
- * weights of the arcs inside the tile, plus eps, rounded to float */
-/* One item of the mixed pass.  FP32 arithmetic for the vector updates and
- * the stencil (IEEE round-to-nearest per operation), FP64-accurate dots
- * (dot4_df per thread, FP64 tree across the item): acc[0] r.z of the
- * updated residual (when not fresh), acc[1] p.q, acc[2] z.q, acc[3]
- * q.(M^-1 q).  The residual plane holds r; z = M^-1 r is formed on the fly
- * with M^-1 = rcp_pre(diag32) of the staged weights. */
-__device__ __forceinline__ void compute_s(const TileDesc &T, int li, float *pnew_all,
-                                          float *rnew_all, float *qnew_all, float *dx_all,
-                                          bool first, bool fresh, float alphaf, float betaf,
-                                          const char *stage, float *Pn, double acc[kNComp])
+/* One item of the mixed pass, in two halves around the consumer barrier.
+ * FP32 arithmetic for the vector updates and the stencil (IEEE
+ * round-to-nearest per operation), FP64-accurate dots (dot4_df per thread):
+ * acc[0] r.z of the updated residual (when not fresh), acc[1] p.q, acc[2]
+ * z.q, acc[3] q.(M^-1 q).  The residual plane holds r; z = M^-1 r is formed
+ * on the fly with M^-1 = rcp_pre(diag32) of the staged weights.
+ * compute_s1: the previous iteration's update and the fold p' = z' + beta
+ * p_old of the own pixels and the halo ring, into Pn; only z' and M^-1 of
+ * the own pixels stay in registers for compute_s2, which computes q = A p'
+ * from Pn and the staged weights. */
+struct ItemS {
+    const float *R, *Q, *PO, *WR, *WD, *DX;
+    int r0b, c0b, ty, tx, r, c0, so, sd;
+    bool own;
+    size_t o;
+};
+
+__device__ __forceinline__ ItemS item_s(const TileDesc &T, int li, const char *stage)
 {
-    const int r0b = (li / T.nbx) * kItemBy, c0b = (li % T.nbx) * kItemBx;
-    const float *R = (const float *)(stage + StageS::oZ);
-    const float *Q = (const float *)(stage + StageS::oQ);
-    const float *PO = (const float *)(stage + StageS::oPO);
-    const float *WR = (const float *)(stage + StageS::oWR);
-    const float *WD = (const float *)(stage + StageS::oWD);
-    const float *DX = (const float *)(stage + StageS::oDX);
-    const int nr = T.nr, nc = T.nc;
-    const int ty = threadIdx.x / kItemTx, tx = threadIdx.x % kItemTx;
-    const int r = r0b + ty, c0 = c0b + tx * kItemVx;
-    const bool own = r < nr && c0 < nc;
+    ItemS I;
+    I.r0b = (li / T.nbx) * kItemBy;
+    I.c0b = (li % T.nbx) * kItemBx;
+    I.R = (const float *)(stage + StageS::oZ);
+    I.Q = (const float *)(stage + StageS::oQ);
+    I.PO = (const float *)(stage + StageS::oPO);
+    I.WR = (const float *)(stage + StageS::oWR);
+    I.WD = (const float *)(stage + StageS::oWD);
+    I.DX = (const float *)(stage + StageS::oDX);
+    I.ty = threadIdx.x / kItemTx;
+    I.tx = threadIdx.x % kItemTx;
+    I.r = I.r0b + I.ty;
+    I.c0 = I.c0b + I.tx * kItemVx;
+    I.own = I.r < T.nr && I.c0 < T.nc;
     /* halo-box coordinates: row i <-> pixel row r0b - 1 + i (the down-arc
      * box starts one row higher: its row i + 1 holds row r0b - 1 + i),
      * column jc <-> c0b - 4 + jc */
-    const int so = (ty + 1) * kSegW + 4 + tx * kItemVx;
-    const int sd = so + kSegW;                 /* wd(r, c) in the down-arc box */
-    /* only z' and M^-1 of the own pixels stay in registers across the
-     * barrier; p' and the weights are read back from shared memory */
-    float zn[4] = {0.f, 0.f, 0.f, 0.f}, rd[4] = {0.f, 0.f, 0.f, 0.f};
-    const size_t o = T.pix + (size_t)r * T.pitch + c0;
-    {
-        float pn[4] = {0.f, 0.f, 0.f, 0.f};
-        if (own) {
-            float wdn[4], wup[4], wrt[4];
-            sld4(WD + sd, wdn);
-            sld4(WD + sd - kSegW, wup);
-            sld4(WR + so, wrt);
-            const float wlf = WR[so - 1];
-            float rv[4], qv[4] = {0.f, 0.f, 0.f, 0.f}, pv[4] = {0.f, 0.f, 0.f, 0.f};
-            float dxv[4] = {0.f, 0.f, 0.f, 0.f};
-            sld4(R + so, rv);
-            if (!fresh) {
-                sld4(Q + so, qv);
-                sld4(DX + ty * kItemBx + tx * kItemVx, dxv);
-            }
-            if (!first) sld4(PO + so, pv);
-#pragma unroll
-            for (int j = 0; j < kItemVx; ++j) {
-                const int c = c0 + j;
-                if (c >= nc) {
-                    rv[j] = 0.f;
-                    continue;
-                }
-                rd[j] = rcp_pre(diag32(r, c, nr, nc, wdn[j], wup[j], wrt[j],
-                                       j == 0 ? wlf : wrt[j - 1]));
-                if (!fresh) {
-                    rv[j] = __fmaf_rn(-alphaf, qv[j], rv[j]);
-                    dxv[j] = __fmaf_rn(alphaf, pv[j], dxv[j]);
-                }
-                zn[j] = __fmul_rn(rv[j], rd[j]);
-                pn[j] = first ? zn[j] : __fmaf_rn(betaf, pv[j], zn[j]);
-            }
-            if (!fresh) {
-                acc[0] = dot4_df(rv, zn);
-                st4(dx_all + o, dxv);
-                st4(rnew_all + o, rv);
-            }
+    I.so = (I.ty + 1) * kSegW + 4 + I.tx * kItemVx;
+    I.sd = I.so + kSegW;                 /* wd(r, c) in the down-arc box */
+    I.o = T.pix + (size_t)I.r * T.pitch + I.c0;
+    return I;
+}
+
+__device__ __forceinline__ void compute_s1(const TileDesc &T, const ItemS &I, float *rnew_all,
+                                           float *dx_all, bool first, bool fresh, float alphaf,
+                                           float betaf, float *Pn, float zn[4], float rd[4],
+                                           double acc[kNComp])
+{
+    const int nr = T.nr, nc = T.nc;
+    float pn[4] = {0.f, 0.f, 0.f, 0.f};
+    if (I.own) {
+        float wdn[4], wup[4], wrt[4];
+        sld4(I.WD + I.sd, wdn);
+        sld4(I.WD + I.sd - kSegW, wup);
+        sld4(I.WR + I.so, wrt);
+        const float wlf = I.WR[I.so - 1];
+        float rv[4], qv[4] = {0.f, 0.f, 0.f, 0.f}, pv[4] = {0.f, 0.f, 0.f, 0.f};
+        float dxv[4] = {0.f, 0.f, 0.f, 0.f};
+        sld4(I.R + I.so, rv);
+        if (!fresh) {
+            sld4(I.Q + I.so, qv);
+            sld4(I.DX + I.ty * kItemBx + I.tx * kItemVx, dxv);
         }
+        if (!first) sld4(I.PO + I.so, pv);
 #pragma unroll
-        for (int j = 0; j < kItemVx; ++j) Pn[so + j] = pn[j];
+        for (int j = 0; j < kItemVx; ++j) {
+            const int c = I.c0 + j;
+            if (c >= nc) {
+                rv[j] = 0.f;
+                continue;
+            }
+            rd[j] = rcp_pre(diag32(I.r, c, nr, nc, wdn[j], wup[j], wrt[j],
+                                   j == 0 ? wlf : wrt[j - 1]));
+            if (!fresh) {
+                rv[j] = __fmaf_rn(-alphaf, qv[j], rv[j]);
+                dxv[j] = __fmaf_rn(alphaf, pv[j], dxv[j]);
+            }
+            zn[j] = __fmul_rn(rv[j], rd[j]);
+            pn[j] = first ? zn[j] : __fmaf_rn(betaf, pv[j], zn[j]);
+        }
+        if (!fresh) {
+            acc[0] = dot4_df(rv, zn);
+            st4(dx_all + I.o, dxv);
+            st4(rnew_all + I.o, rv);
+        }
     }
+#pragma unroll
+    for (int j = 0; j < kItemVx; ++j) Pn[I.so + j] = pn[j];
     /* halo ring: the same update and fold, so neighbours agree bit for bit */
     if (threadIdx.x < 2 * kItemBx + 2 * kItemBy) {
         int h = threadIdx.x, i, jc;
@@ -855,55 +867,60 @@ __device__ __forceinline__ void compute_s(const TileDesc &T, int li, float *pnew
         else if (h < 2 * kItemBx) { i = kItemBy + 1; jc = 4 + h - kItemBx; }
         else if (h < 2 * kItemBx + kItemBy) { i = 1 + h - 2 * kItemBx; jc = 3; }
         else { i = 1 + h - 2 * kItemBx - kItemBy; jc = 4 + kItemBx; }
-        const int gr = r0b - 1 + i, gc = c0b - 4 + jc;
+        const int gr = I.r0b - 1 + i, gc = I.c0b - 4 + jc;
         float v = 0.f;
         if (gr >= 0 && gr < nr && gc >= 0 && gc < nc) {
             const int sidx = i * kSegW + jc;
-            const float m = rcp_pre(diag32(gr, gc, nr, nc, WD[sidx + kSegW], WD[sidx], WR[sidx],
-                                           WR[sidx - 1]));
-            const float rr = fresh ? R[sidx] : __fmaf_rn(-alphaf, Q[sidx], R[sidx]);
+            const float m = rcp_pre(diag32(gr, gc, nr, nc, I.WD[sidx + kSegW], I.WD[sidx],
+                                           I.WR[sidx], I.WR[sidx - 1]));
+            const float rr = fresh ? I.R[sidx] : __fmaf_rn(-alphaf, I.Q[sidx], I.R[sidx]);
             const float z = __fmul_rn(rr, m);
-            v = first ? z : __fmaf_rn(betaf, PO[sidx], z);
+            v = first ? z : __fmaf_rn(betaf, I.PO[sidx], z);
         }
         Pn[i * kSegW + jc] = v;
     }
-    __syncthreads();
-    if (own) {
-        float pn[4], up[4], dn[4], wdn[4], wup[4], wrt[4], qv[4] = {0.f, 0.f, 0.f, 0.f};
-        sld4(Pn + so, pn);
-        sld4(Pn + so - kSegW, up);
-        sld4(Pn + so + kSegW, dn);
-        const float lf = Pn[so - 1], rt = Pn[so + 4];
-        sld4(WD + sd, wdn);
-        sld4(WD + sd - kSegW, wup);
-        sld4(WR + so, wrt);
-        const float wlf = WR[so - 1];
-        float mq[4] = {0.f, 0.f, 0.f, 0.f};
+}
+
+__device__ __forceinline__ void compute_s2(const TileDesc &T, const ItemS &I, float *pnew_all,
+                                           float *qnew_all, const float *Pn, const float zn[4],
+                                           const float rd[4], double acc[kNComp])
+{
+    if (!I.own) return;
+    const int nr = T.nr, nc = T.nc, r = I.r, so = I.so;
+    float pn[4], up[4], dn[4], wdn[4], wup[4], wrt[4], qv[4] = {0.f, 0.f, 0.f, 0.f};
+    sld4(Pn + so, pn);
+    sld4(Pn + so - kSegW, up);
+    sld4(Pn + so + kSegW, dn);
+    const float lf = Pn[so - 1], rt = Pn[so + 4];
+    sld4(I.WD + I.sd, wdn);
+    sld4(I.WD + I.sd - kSegW, wup);
+    sld4(I.WR + so, wrt);
+    const float wlf = I.WR[so - 1];
+    float mq[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-        for (int j = 0; j < kItemVx; ++j) {
-            const int c = c0 + j;
-            if (c >= nc) {
-                pn[j] = 0.f;
-                continue;
-            }
-            const float xl = j == 0 ? lf : pn[j - 1];
-            const float xr = j == kItemVx - 1 ? rt : pn[j + 1];
-            const float wl = j == 0 ? wlf : wrt[j - 1];
-            const float xa = pn[j];
-            float y = __fmul_rn(kLapEpsF, xa);
-            if (r < nr - 1) y = __fmaf_rn(wdn[j], __fsub_rn(xa, dn[j]), y);
-            if (r > 0)      y = __fmaf_rn(wup[j], __fsub_rn(xa, up[j]), y);
-            if (c < nc - 1) y = __fmaf_rn(wrt[j], __fsub_rn(xa, xr), y);
-            if (c > 0)      y = __fmaf_rn(wl, __fsub_rn(xa, xl), y);
-            qv[j] = y;
-            mq[j] = __fmul_rn(y, rd[j]);
+    for (int j = 0; j < kItemVx; ++j) {
+        const int c = I.c0 + j;
+        if (c >= nc) {
+            pn[j] = 0.f;
+            continue;
         }
-        acc[1] = dot4_df(pn, qv);
-        acc[2] = dot4_df(zn, qv);
-        acc[3] = dot4_df(qv, mq);
-        st4(pnew_all + o, pn);
-        st4(qnew_all + o, qv);
+        const float xl = j == 0 ? lf : pn[j - 1];
+        const float xr = j == kItemVx - 1 ? rt : pn[j + 1];
+        const float wl = j == 0 ? wlf : wrt[j - 1];
+        const float xa = pn[j];
+        float y = __fmul_rn(kLapEpsF, xa);
+        if (r < nr - 1) y = __fmaf_rn(wdn[j], __fsub_rn(xa, dn[j]), y);
+        if (r > 0)      y = __fmaf_rn(wup[j], __fsub_rn(xa, up[j]), y);
+        if (c < nc - 1) y = __fmaf_rn(wrt[j], __fsub_rn(xa, xr), y);
+        if (c > 0)      y = __fmaf_rn(wl, __fsub_rn(xa, xl), y);
+        qv[j] = y;
+        mq[j] = __fmul_rn(y, rd[j]);
     }
+    acc[1] = dot4_df(pn, qv);
+    acc[2] = dot4_df(zn, qv);
+    acc[3] = dot4_df(qv, mq);
+    st4(pnew_all + I.o, pn);
+    st4(qnew_all + I.o, qv);
 }
 
 /* mixed precision: fold the FP32 increment into the FP64 solution, optionally
@@ -913,7 +930,7 @@ __device__ void phase_fold(const TileDesc &T, int li, const SolverPlanes &P, con
                            bool with_update, double alpha)
 {
     ItemXY q = item_xy(T, li);
-    if (q.r >= T.nr || q.c0 >= T.nc) return;
+    if (threadIdx.x >= kItemThreads || q.r >= T.nr || q.c0 >= T.nc) return;
     const size_t o = T.pix + (size_t)q.r * T.pitch + q.c0;
     float dxv[4], pv[4];
     double xv[4];
@@ -937,7 +954,7 @@ template <typename V>
 __device__ void phase_rw(const TileDesc &T, int li, const SolverPlanes &P, float delta)
 {
     ItemXY q = item_xy(T, li);
-    if (q.r >= T.nr || q.c0 >= T.nc) return;
+    if (threadIdx.x >= kItemThreads || q.r >= T.nr || q.c0 >= T.nc) return;
     const double *x = P.x + T.pix;
     const double dd = (double)delta * (double)delta;
     const int r = q.r, nr = T.nr, nc = T.nc, pitch = T.pitch, pp = T.ph_pitch;
@@ -977,7 +994,7 @@ template <typename V>
 __device__ void phase_final(const TileDesc &T, int li, const SolverPlanes &P)
 {
     ItemXY q = item_xy(T, li);
-    if (q.r >= T.nr || q.c0 >= T.nc) return;
+    if (threadIdx.x >= kItemThreads || q.r >= T.nr || q.c0 >= T.nc) return;
     const double *x = P.x + T.pix;
     double off = (double)__ldg(T.ph) - ldc(x);
     size_t prow = (size_t)q.r * T.pitch;
@@ -1233,63 +1250,119 @@ __device__ void run_pass(const SliceCtl &sc, const TileDesc *gt, const TileState
     __syncthreads();
 }
 
-/* the mixed single-synchronisation pass over this block's slice, staged
- * like run_pass, with kNComp partials per item */
+/* The mixed pass runs warp-specialised: the block's last warp is the
+ * producer (one lane issues every item's TMA boxes into the NS-stage ring,
+ * waiting on the stage's "empty" barrier before refilling it), the other
+ * kItemThreads threads consume items in the same order (wait on the stage's
+ * "full" barrier, compute, arrive on "empty").  The consumers synchronise
+ * among themselves once per item, with a named barrier between the two
+ * halves of an item (the fold writes Pn, the stencil reads neighbours'
+ * values); Pn and the warp partials alternate between two buffers by item
+ * parity.  The cross-warp sum of item k's partials and their store run in
+ * warp 0 after the barrier of item k+1, when every warp has finished item
+ * k, so no second barrier per item is needed.  kk counts the ring's items
+ * over the whole launch (stage = kk mod NS, use = kk / NS), identically in
+ * every thread.  Tile totals of the pass are formed at its end, for every
+ * tile of the block's slice. */
+constexpr int kConsumerBar = 1;
+__device__ __forceinline__ void consumer_sync()
+{
+    asm volatile("bar.sync %0, %1;" ::"n"(kConsumerBar), "n"(kItemThreads) : "memory");
+}
+
+/* cross-warp sum (fixed tree, the same as block_sum4_item's warp-0 stage) of
+ * one item's warp partials, stored as the item's partials */
+__device__ __forceinline__ void store_item4(const double (*red)[8], double *part, int nitems,
+                                            int item)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int c = 0; c < kNComp; ++c) {
+        double x = lane < kItemThreads / 32 ? red[c][lane] : 0.0;
+        for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+        if (lane == 0) part[(size_t)c * nitems + item] = x;
+    }
+}
+
 template <int NS>
 __device__ void run_pass_s(const SliceCtl &sc, const TileDesc *gt, const TileState *st, int ntiles,
                            int nitems, const SolveMaps &M, int zsel, int ksel, bool first,
-                           bool fresh, float *pnew, float *znew, float *qnew, float *dx,
+                           bool fresh, float *pnew, float *rnew, float *qnew, float *dx,
                            double *part, double *tot, unsigned *cnt, double *sw,
-                           double (*sw4)[kNComp][8], double *s_bcast, int *s_flag, float *Pn,
-                           char *stages, uint64_t *bars, uint32_t &parity, SolverCtl *ctl,
-                           long long timeout_ns)
+                           double (*red)[kNComp][8], double *s_bcast, int *s_flag, float *Pn2,
+                           char *stages, uint64_t *full, uint64_t *empty, uint32_t &kk,
+                           SolverCtl *ctl, long long timeout_ns)
 {
     constexpr size_t SB = stage_bytes<float>();
-    if (sc.s0 >= sc.s1) return;
-    Cursor ci = cursor_active(Cursor{sc.s0, sc.t0}, sc, gt, st, ntiles);
-    if (ci.p >= sc.s1) return;
-    Cursor cc = ci;
-    if (threadIdx.x == 0) {
-        fence_async_global();
-        fence_async_smem();
+    constexpr size_t PNE = pn_bytes<float>() / sizeof(float);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t nit = 0;
+    if (sc.s0 < sc.s1) {
+        for (Cursor c = cursor_active(Cursor{sc.s0, sc.t0}, sc, gt, st, ntiles); c.p < sc.s1;
+             c = cursor_active(Cursor{c.p + 1, c.t}, sc, gt, st, ntiles))
+            ++nit;
     }
-    for (int k = 0; k < NS && ci.p < sc.s1; ++k) {
-        if (threadIdx.x == 0)
-            issue_s(stile(sc, gt, ci.t), ci.p - sc.pre[ci.t], M, zsel, ksel, first, fresh,
-                    stages + k * SB, bars + k);
-        ci = cursor_active(Cursor{ci.p + 1, ci.t}, sc, gt, st, ntiles);
-    }
-    int done = 0;
-    while (cc.p < sc.s1) {
-        int s = done % NS;
-        mbar_wait(bars + s, (parity >> s) & 1u, ctl, timeout_ns);
-        parity ^= 1u << s;
-        ++done;
-        const TileDesc &T = stile(sc, gt, cc.t);
-        int li = cc.p - sc.pre[cc.t];
-        double acc[kNComp] = {0.0, 0.0, 0.0, 0.0};
-        compute_s(T, li, pnew, znew, qnew, dx, first, fresh, (float)salpha(sc, st, cc.t),
-                  (float)sbeta(sc, st, cc.t), stages + s * SB, Pn, acc);
-        block_sum4_item(acc, sw4, done & 1);   /* contains the item barrier */
-        if (threadIdx.x == 0) {
-#pragma unroll
-            for (int c = 0; c < kNComp; ++c) part[(size_t)c * nitems + T.item0 + li] = acc[c];
-            if (ci.p < sc.s1) {
-                fence_async_smem();
-                issue_s(stile(sc, gt, ci.t), ci.p - sc.pre[ci.t], M, zsel, ksel, first, fresh,
-                        stages + s * SB, bars + s);
+    if (nit > 0) {
+        if (warp == kItemThreads / 32) {
+            /* producer */
+            if (lane == 0) {
+                fence_async_global();
+                uint32_t k = kk;
+                for (Cursor c = cursor_active(Cursor{sc.s0, sc.t0}, sc, gt, st, ntiles);
+                     c.p < sc.s1; c = cursor_active(Cursor{c.p + 1, c.t}, sc, gt, st, ntiles), ++k) {
+                    const uint32_t s = k % NS, use = k / NS;
+                    if (use > 0) mbar_wait(empty + s, (use - 1) & 1u, ctl, timeout_ns);
+                    fence_async_smem();
+                    issue_s(stile(sc, gt, c.t), c.p - sc.pre[c.t], M, zsel, ksel, first, fresh,
+                            stages + s * SB, full + s);
+                }
             }
+        } else {
+            /* consumers */
+            uint32_t k = kk;
+            int prev = -1;   /* partial index of the previous item */
+            for (Cursor c = cursor_active(Cursor{sc.s0, sc.t0}, sc, gt, st, ntiles); c.p < sc.s1;
+                 c = cursor_active(Cursor{c.p + 1, c.t}, sc, gt, st, ntiles), ++k) {
+                const uint32_t s = k % NS;
+                mbar_wait(full + s, (k / NS) & 1u, ctl, timeout_ns);
+                const TileDesc &T = stile(sc, gt, c.t);
+                const int li = c.p - sc.pre[c.t];
+                const ItemS I = item_s(T, li, stages + s * SB);
+                float *Pn = Pn2 + (k & 1u) * PNE;
+                double acc[kNComp] = {0.0, 0.0, 0.0, 0.0};
+                float zn[4] = {0.f, 0.f, 0.f, 0.f}, rd[4] = {0.f, 0.f, 0.f, 0.f};
+                compute_s1(T, I, rnew, dx, first, fresh, (float)salpha(sc, st, c.t),
+                           (float)sbeta(sc, st, c.t), Pn, zn, rd, acc);
+                consumer_sync();
+                if (warp == 0 && prev >= 0) store_item4(red[(k - 1) & 1u], part, nitems, prev);
+                compute_s2(T, I, pnew, qnew, Pn, zn, rd, acc);
+#pragma unroll
+                for (int cc = 0; cc < kNComp; ++cc)
+                    for (int off = 16; off > 0; off >>= 1)
+                        acc[cc] += __shfl_down_sync(0xffffffffu, acc[cc], off);
+                if (lane == 0) {
+#pragma unroll
+                    for (int cc = 0; cc < kNComp; ++cc) red[k & 1u][cc][warp] = acc[cc];
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(empty + s);
+                prev = T.item0 + li;
+            }
+            consumer_sync();
+            if (warp == 0) store_item4(red[(k - 1) & 1u], part, nitems, prev);
         }
-        if (ci.p < sc.s1) ci = cursor_active(Cursor{ci.p + 1, ci.t}, sc, gt, st, ntiles);
-        Cursor nx = cursor_active(Cursor{cc.p + 1, cc.t}, sc, gt, st, ntiles);
-        if (nx.p >= sc.s1 || nx.t != cc.t) {
-            int a, b;
-            slice_items(sc, T, cc.t, a, b);
-            seg_done4(T, cc.t, b - a, part, nitems, tot, ntiles, cnt, sw, s_bcast, s_flag);
-        }
-        cc = nx;
     }
+    kk += nit;
     __syncthreads();
+    if (nit == 0) return;
+    /* the block's partials of every active tile of its slice are stored */
+    for (int t = sc.t0; t <= sc.t1; ++t) {
+        if (sc.pre[t + 1] == sc.pre[t] || !sactive(sc, st, t)) continue;
+        const TileDesc &T = stile(sc, gt, t);
+        int a, b;
+        slice_items(sc, T, t, a, b);
+        if (b > a) seg_done4(T, t, b - a, part, nitems, tot, ntiles, cnt, sw, s_bcast, s_flag);
+    }
 }
 
 /* state written by other blocks before the last grid barrier: read from L2 */
@@ -1359,17 +1432,17 @@ __device__ __forceinline__ void carry_inactive(const TileState *from, TileState 
  * side, optional warm start, no anchoring); a separate instantiation so the
  * main path's register allocation does not carry its extra inputs */
 template <typename V, bool WLS, int NS, int MINB>
-__global__ void __launch_bounds__(kItemThreads, MINB)
+__global__ void __launch_bounds__(solve_threads<V>()) __maxnreg__((solve_regs<V, MINB>()))
     k_solve(const TileDesc *__restrict__ tiles, const int *__restrict__ item_tile, int nitems,
             int ntiles, SolverPlanes P, TileState *st, double *part, SolverCtl *ctl,
             SolveParams sp, long long timeout_ns, const __grid_constant__ SolveMaps M)
 {
     extern __shared__ __align__(128) char dsm_raw[];
     __shared__ double sw[32];
-    __shared__ double sw4[2][kNComp][8];
+    __shared__ double red[2][kNComp][8];   /* mixed: warp partials by item parity */
     __shared__ double s_bcast;
     __shared__ int s_flag;
-    __shared__ __align__(8) uint64_t bars[NS];
+    __shared__ __align__(8) uint64_t bars[2 * NS];   /* ring: full [0, NS), empty [NS, 2 NS) */
     __shared__ SliceCtl sc;
     char *dsm = (char *)(((uintptr_t)dsm_raw + 127) & ~(uintptr_t)127);
     constexpr bool mixed = sizeof(V) == 4;
@@ -1386,10 +1459,14 @@ __global__ void __launch_bounds__(kItemThreads, MINB)
     /* z buffers: the first is written by the assembly; mixed mode
      * double-buffers z in the r plane (r = z diag is not stored) */
     V *zb[2] = {(V *)P.z, (V *)P.r};
-    uint32_t parity = 0u;
+    uint32_t parity = 0u;   /* FP64 ring: phase bit per stage */
+    uint32_t kk = 0u;       /* mixed ring: items so far */
     (void)item_tile;
     if (threadIdx.x == 0) {
-        for (int k = 0; k < NS; ++k) mbar_init(&bars[k]);
+        for (int k = 0; k < NS; ++k) {
+            mbar_init(&bars[k]);
+            mbar_init_n(&bars[NS + k], kItemThreads / 32);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -1589,8 +1666,9 @@ __global__ void __launch_bounds__(kItemThreads, MINB)
                 }
                 run_pass_s<NS>(sc, tiles, st + (size_t)cur * ntiles, ntiles, nitems, M, zsel, k & 1,
                            k == 0, fresh, (float *)pb[(k + 1) & 1], (float *)zb[zsel ^ 1],
-                           qb[(k + 1) & 1], P.dx, pbuf[pc & 1], tbuf[pc & 1], tick, sw, sw4,
-                           &s_bcast, &s_flag, (float *)Pn, dsm, bars, parity, ctl, timeout_ns);
+                           qb[(k + 1) & 1], P.dx, pbuf[pc & 1], tbuf[pc & 1], tick, sw, red,
+                           &s_bcast, &s_flag, (float *)Pn, dsm, bars, bars + NS, kk, ctl,
+                           timeout_ns);
                 ++pc;
                 if (!fresh) zsel ^= 1;
                 prev_fresh = fresh;
@@ -1722,14 +1800,14 @@ static int launch_solve_shape(const TileDesc *tiles, const int *item_tile, int n
     auto kern = k_solve<V, WLS, NS, MINB>;
     CUPHU_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)smem));
-    CUPHU_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kItemThreads,
-                                                                 smem));
+    constexpr int BT = solve_threads<V>();
+    CUPHU_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BT, smem));
     if (per_sm < 1) return fail(CUPHU_ERR_CUDA, "solver kernel cannot be resident");
     per_sm = std::min(per_sm, MINB);
     int grid = std::min(nsm * per_sm, std::max(nitems, 1));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(kItemThreads);
+    cfg.blockDim = dim3(BT);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
@@ -1758,9 +1836,9 @@ static int launch_solve_kernel(const TileDesc *tiles, const int *item_tile, int 
                                                 rows, st, part, ctl, sp, timeout_ns, device, s)
     if constexpr (sizeof(V) == 4) {
         switch (v) {
-        case 1: CUPHU_SOLVE_SHAPE(3, 2);
-        case 2: CUPHU_SOLVE_SHAPE(2, 2);
-        default: CUPHU_SOLVE_SHAPE(2, 3);
+        case 1: CUPHU_SOLVE_SHAPE(2, 2);
+        case 2: CUPHU_SOLVE_SHAPE(5, 1);
+        default: CUPHU_SOLVE_SHAPE(3, 2);
         }
     } else {
         switch (v) {
@@ -1775,7 +1853,7 @@ int solve_shape_count(bool fp64) { return fp64 ? 2 : 3; }
 
 void solve_shape_of(bool fp64, int v, int *stages, int *blocks_per_sm)
 {
-    static const int mixed[3][2] = {{2, 3}, {3, 2}, {2, 2}};
+    static const int mixed[3][2] = {{3, 2}, {2, 2}, {5, 1}};
     static const int f64[2][2] = {{2, 2}, {3, 1}};
     const int(*t)[2] = fp64 ? f64 : mixed;
     const int n = solve_shape_count(fp64);

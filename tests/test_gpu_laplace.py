@@ -7,7 +7,7 @@
   cycle maps with at most a handful of mismatches (all at pixels whose
   continuous solution sits within a hair of a half cycle).
 * The reference FP32 kernels (float-atomic dot products, nondeterministic)
-  are compared by cycle-map agreement fraction.
+  are compared against their own run-to-run spread of the cycle map.
 """
 import ctypes as C
 
@@ -88,15 +88,30 @@ def test_solver_is_deterministic(torch_cuda):
         assert np.array_equal(a[2].view(np.int32), b[2].view(np.int32))
 
 
-def test_against_reference_fp32_kernels(torch_cuda):
+@pytest.mark.parametrize("shape,seed", [((128, 128), 9), ((256, 256), 5), ((384, 300), 3),
+                                        ((512, 512), 0)])
+def test_against_reference_fp32_kernels(torch_cuda, shape, seed):
+    """The reference's Laplace kernels (FP32 vectors; dot products reduced
+    with float atomicAdd, so their order varies between runs) against this
+    build's FP64 and mixed solves on the same SMOOTH costs (the reference's
+    Laplace entry takes SMOOTH costs only).  The bar is the reference's own
+    run-to-run spread: it runs several times, and this build's cycle map may
+    differ from any one run in no more pixels than the farthest other run
+    does.  Where every reference run agrees, the maps must be identical."""
     if O.ref_lib() is None:
         pytest.skip("reference kernels not built")
-    ph, g, _ = scene(128, 128, 9)
+    ph, g, _ = scene(*shape, seed)
     costs = O.build_costs(ph, g, 5.0, mode=0)
-    ref_unw, _ = O.ref_laplace(costs, ph)
-    gu, gk, _, _ = gpu_solve(torch_cuda, costs, ph, precision=0, n_irls=16)
-    kref = np.rint((ref_unw.astype(np.float64) - ph) / (2 * np.pi))
-    assert np.mean(kref != gk) < 0.02
+    runs = []
+    for _ in range(6):
+        unw, _ = O.ref_laplace(costs, ph)
+        runs.append(np.rint((unw.astype(np.float64) - ph) / (2 * np.pi)).astype(np.int64))
+    floor = [max(int(np.sum(a != b)) for j, b in enumerate(runs) if j != i)
+             for i, a in enumerate(runs)]
+    for prec in (1, 0):
+        _, gk, _, _ = gpu_solve(torch_cuda, costs, ph, precision=prec, n_irls=16)
+        mism = [int(np.sum(gk != k)) for k in runs]
+        assert all(m <= f for m, f in zip(mism, floor)), (prec, mism, floor)
 
 
 def test_max_iter_cap_and_zero_weights(torch_cuda):
