@@ -1104,9 +1104,11 @@ int cuphu_autotune(const float *igram_c64, const float *corr, int nrow, int ncol
     long long items = 0;
     CuPhuSolveOptions so0;
     default_solve_options(&so0);
-    const int nshape = solve_shape_count(so0.precision == CUPHU_PREC_FP64);
+    const bool fp64 = so0.precision == CUPHU_PREC_FP64;
+    const int kind = fp64 ? 2 : 1;
+    const int nshape = solve_shape_count(fp64);
     for (int v = 0; v < nshape && !rc; ++v) {
-        tune_force(1, v);
+        tune_force(kind, v);
         CuPhuSolveOptions so = so0;
         so.max_iter = 20;
         so.n_irls = 0;
@@ -1118,8 +1120,8 @@ int cuphu_autotune(const float *igram_c64, const float *corr, int nrow, int ncol
         items = tune_probe_items();
         if (!rc && st.solve_ms < best_ms) { best_ms = (float)st.solve_ms; best_shape = v; }
     }
-    tune_force(1, -1);
-    if (!rc && items > 0) tune_set(gpu_id, 1, items, best_shape);
+    tune_force(kind, -1);
+    if (!rc && items > 0) tune_set(gpu_id, kind, items, best_shape);
     cudaError_t e = cudaStreamSynchronize(s);
     cudaFreeAsync(d_ig, s); cudaFreeAsync(d_corr, s); cudaFreeAsync(d_ph, s);
     cudaFreeAsync(d_unw, s); cudaFreeAsync(d_cost, s);
@@ -1302,6 +1304,7 @@ int cuphu_test_force_solve_shape(int shape)
     if (shape < -1 || shape >= std::max(solve_shape_count(false), solve_shape_count(true)))
         return fail(CUPHU_ERR_INVALID, "no such solver launch shape");
     tune_force(1, shape);
+    tune_force(2, shape);
     return 0;
 }
 

@@ -1830,7 +1830,7 @@ static int launch_solve_kernel(const TileDesc *tiles, const int *item_tile, int 
         return fail(CUPHU_ERR_INVALID, "at most 1024 tiles per solver launch");
     /* the shape from the autotuner (job size = item count) */
     tune_note_items(nitems);
-    const int v = tune_get(device, 1, (long long)nitems);
+    const int v = tune_get(device, sizeof(V) == 8 ? 2 : 1, (long long)nitems);
 #define CUPHU_SOLVE_SHAPE(NS, MINB)                                                            \
     return launch_solve_shape<V, WLS, NS, MINB>(tiles, item_tile, nitems, ntiles, P, pitch,    \
                                                 rows, st, part, ctl, sp, timeout_ns, device, s)

@@ -15,11 +15,13 @@
 
 namespace cuphu {
 namespace {
-constexpr int kDevs = 64, kKinds = 2, kClasses = 48;
+/* kinds: 0 cost kernel variant, 1 mixed-precision solver shape, 2 FP64
+ * solver shape (the shape indices of the two precisions differ) */
+constexpr int kDevs = 64, kKinds = 3, kClasses = 48;
 std::mutex g_tune_mu;
 int g_tune[kDevs][kKinds][kClasses];
 bool g_tune_init = false;
-thread_local int g_force[kKinds] = {-1, -1};
+thread_local int g_force[kKinds] = {-1, -1, -1};
 thread_local long long g_probe_items = 0;
 
 void init_locked()
