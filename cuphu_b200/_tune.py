@@ -12,7 +12,7 @@ from ._lib import check, default_params, default_tile_params, lib, ptr
 
 _COST = {"smooth": 0, "defo": 1, "topo": 2}
 # the mixed-precision solver's launch shapes, in the library's index order
-_SOLVE_SHAPES = ((3, 2), (2, 2), (5, 1))
+_SOLVE_SHAPES = ((3, 2), (2, 2), (6, 1))
 
 
 def autotune(igram, corr, nlooks, cost="smooth", ntiles=(1, 1), tile_overlap=(0, 0), gpu_id=0):

@@ -291,6 +291,38 @@ __device__ __forceinline__ double dot4_df(const float a[4], const float b[4])
     return (double)hi + (double)lo;
 }
 
+/* paired FP32 arithmetic (two lanes per instruction, IEEE round-to-nearest
+ * per lane, the same results as the scalar operations) */
+__device__ __forceinline__ float2 pf2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 psub(float2 a, float2 b)   /* a - b, one rounding */
+{
+    return __ffma2_rn(b, pf2(-1.0f, -1.0f), a);
+}
+
+/* two dot4_df sums at once, lane 0 for (a0, b0) and lane 1 for (a1, b1):
+ * the same operations, so each result equals dot4_df's */
+__device__ __forceinline__ void dot4_df2(const float a0[4], const float b0[4], const float a1[4],
+                                         const float b1[4], double &r0, double &r1)
+{
+    float2 a = pf2(a0[0], a1[0]), b = pf2(b0[0], b1[0]);
+    float2 hi = __fmul2_rn(a, b);
+    float2 lo = __ffma2_rn(a, b, pf2(-hi.x, -hi.y));
+#pragma unroll
+    for (int j = 1; j < 4; ++j) {
+        a = pf2(a0[j], a1[j]);
+        b = pf2(b0[j], b1[j]);
+        const float2 p = __fmul2_rn(a, b);
+        const float2 e = __ffma2_rn(a, b, pf2(-p.x, -p.y));
+        const float2 sm = __fadd2_rn(hi, p);
+        const float2 bp = psub(sm, hi);
+        const float2 err = __fadd2_rn(psub(hi, psub(sm, bp)), psub(p, bp));
+        hi = sm;
+        lo = __fadd2_rn(lo, __fadd2_rn(e, err));
+    }
+    r0 = (double)hi.x + (double)lo.x;
+    r1 = (double)hi.y + (double)lo.y;
+}
+
 /* ── INIT / true residual: b, diag (A10) and r = b - A x, rz partial ────────
  * zero_x: first pass (x = 0, r = b).  write_diag: assemble pass (else the
  * stored diag is reused: residual replacement).  FP64 mode: z = r / diag
@@ -303,8 +335,7 @@ __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, b
                              bool write_diag, V *zout)
 {
     ItemXY q = item_xy(T, li);
-    /* the mixed kernel's producer warp owns no pixels */
-    if (threadIdx.x >= kItemThreads || q.r >= T.nr || q.c0 >= T.nc) return 0.0;
+    if (q.r >= T.nr || q.c0 >= T.nc) return 0.0;
     double *x = P.x + T.pix;
     V *rr = (V *)P.r + T.pix;
     V *dg = (V *)P.diag + T.pix;
@@ -493,19 +524,7 @@ template <typename V, int NS> __host__ __device__ constexpr size_t solve_smem_by
     /* mixed mode double-buffers Pn by item parity */
     return NS * stage_bytes<V>() + (sizeof(V) == 4 ? 2 : 1) * pn_bytes<V>() + 128;
 }
-/* threads per block: mixed mode adds the producer warp */
-template <typename V> __host__ __device__ constexpr int solve_threads()
-{
-    return sizeof(V) == 4 ? kItemThreads + 32 : kItemThreads;
-}
-/* registers per thread that let MINB blocks be resident on one SM (65536
- * registers, allocated per thread in multiples of 8), at most 255 */
-template <typename V, int MINB> __host__ __device__ constexpr int solve_regs()
-{
-    return (65536 / (MINB * solve_threads<V>())) / 8 * 8 > 255
-               ? 255
-               : (65536 / (MINB * solve_threads<V>())) / 8 * 8;
-}
+
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p)
 {
@@ -514,16 +533,6 @@ __device__ __forceinline__ uint32_t smem_addr(const void *p)
 __device__ __forceinline__ void mbar_init(uint64_t *bar)
 {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
-}
-/* an mbarrier that completes a phase after `count` plain arrivals */
-__device__ __forceinline__ void mbar_init_n(uint64_t *bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
-                 : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 __device__ __forceinline__ void mbar_expect(uint64_t *bar, uint32_t bytes)
 {
@@ -540,13 +549,16 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, i
         "l"(map), "r"(x), "r"(y), "r"(smem_addr(bar))
         : "memory");
 }
+/* one bounded test of a phase; a thread whose phase is not complete may be
+ * suspended for up to 20 us (the suspend-time hint) instead of returning at
+ * once, so waiting warps do not take issue slots from computing ones */
 __device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity)
 {
     uint32_t ok;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}"
         : "=r"(ok)
-        : "r"(smem_addr(bar)), "r"(parity)
+        : "r"(smem_addr(bar)), "r"(parity), "r"(20000u)
         : "memory");
     return ok != 0;
 }
@@ -787,6 +799,7 @@ struct ItemS {
     const float *R, *Q, *PO, *WR, *WD, *DX;
     int r0b, c0b, ty, tx, r, c0, so, sd;
     bool own;
+    bool in;   /* every pixel of the item has all four arcs inside the tile */
     size_t o;
 };
 
@@ -806,6 +819,7 @@ __device__ __forceinline__ ItemS item_s(const TileDesc &T, int li, const char *s
     I.r = I.r0b + I.ty;
     I.c0 = I.c0b + I.tx * kItemVx;
     I.own = I.r < T.nr && I.c0 < T.nc;
+    I.in = I.r0b >= 1 && I.r0b + kItemBy <= T.nr - 1 && I.c0b >= 1 && I.c0b + kItemBx <= T.nc - 1;
     /* halo-box coordinates: row i <-> pixel row r0b - 1 + i (the down-arc
      * box starts one row higher: its row i + 1 holds row r0b - 1 + i),
      * column jc <-> c0b - 4 + jc */
@@ -836,21 +850,52 @@ __device__ __forceinline__ void compute_s1(const TileDesc &T, const ItemS &I, fl
             sld4(I.DX + I.ty * kItemBx + I.tx * kItemVx, dxv);
         }
         if (!first) sld4(I.PO + I.so, pv);
+        if (I.in) {
+            /* all four arcs in the tile: diag32's sum without the tests (a
+             * weight that is not positive adds +0, which diag32 skips), and
+             * the updates two pixels per instruction */
 #pragma unroll
-        for (int j = 0; j < kItemVx; ++j) {
-            const int c = I.c0 + j;
-            if (c >= nc) {
-                rv[j] = 0.f;
-                continue;
+            for (int j = 0; j < kItemVx; j += 2) {
+                const float2 dn = pf2(fmaxf(wdn[j], 0.f), fmaxf(wdn[j + 1], 0.f));
+                const float2 up = pf2(fmaxf(wup[j], 0.f), fmaxf(wup[j + 1], 0.f));
+                const float2 rt = pf2(fmaxf(wrt[j], 0.f), fmaxf(wrt[j + 1], 0.f));
+                const float2 lf = pf2(fmaxf(j == 0 ? wlf : wrt[j - 1], 0.f), fmaxf(wrt[j], 0.f));
+                const float2 d = __fadd2_rn(__fadd2_rn(__fadd2_rn(__fadd2_rn(dn, up), rt), lf),
+                                            pf2(kLapEpsF, kLapEpsF));
+                const float2 m = pf2(rcp_pre(d.x), rcp_pre(d.y));
+                float2 r2 = pf2(rv[j], rv[j + 1]);
+                const float2 p2 = pf2(pv[j], pv[j + 1]);
+                if (!fresh) {
+                    r2 = __ffma2_rn(pf2(-alphaf, -alphaf), pf2(qv[j], qv[j + 1]), r2);
+                    const float2 x2 = __ffma2_rn(pf2(alphaf, alphaf), p2,
+                                                 pf2(dxv[j], dxv[j + 1]));
+                    dxv[j] = x2.x;
+                    dxv[j + 1] = x2.y;
+                }
+                const float2 z2 = __fmul2_rn(r2, m);
+                const float2 f2v = first ? z2 : __ffma2_rn(pf2(betaf, betaf), p2, z2);
+                rv[j] = r2.x; rv[j + 1] = r2.y;
+                rd[j] = m.x; rd[j + 1] = m.y;
+                zn[j] = z2.x; zn[j + 1] = z2.y;
+                pn[j] = f2v.x; pn[j + 1] = f2v.y;
             }
-            rd[j] = rcp_pre(diag32(I.r, c, nr, nc, wdn[j], wup[j], wrt[j],
-                                   j == 0 ? wlf : wrt[j - 1]));
-            if (!fresh) {
-                rv[j] = __fmaf_rn(-alphaf, qv[j], rv[j]);
-                dxv[j] = __fmaf_rn(alphaf, pv[j], dxv[j]);
+        } else {
+#pragma unroll
+            for (int j = 0; j < kItemVx; ++j) {
+                const int c = I.c0 + j;
+                if (c >= nc) {
+                    rv[j] = 0.f;
+                    continue;
+                }
+                rd[j] = rcp_pre(diag32(I.r, c, nr, nc, wdn[j], wup[j], wrt[j],
+                                       j == 0 ? wlf : wrt[j - 1]));
+                if (!fresh) {
+                    rv[j] = __fmaf_rn(-alphaf, qv[j], rv[j]);
+                    dxv[j] = __fmaf_rn(alphaf, pv[j], dxv[j]);
+                }
+                zn[j] = __fmul_rn(rv[j], rd[j]);
+                pn[j] = first ? zn[j] : __fmaf_rn(betaf, pv[j], zn[j]);
             }
-            zn[j] = __fmul_rn(rv[j], rd[j]);
-            pn[j] = first ? zn[j] : __fmaf_rn(betaf, pv[j], zn[j]);
         }
         if (!fresh) {
             acc[0] = dot4_df(rv, zn);
@@ -897,27 +942,46 @@ __device__ __forceinline__ void compute_s2(const TileDesc &T, const ItemS &I, fl
     sld4(I.WR + so, wrt);
     const float wlf = I.WR[so - 1];
     float mq[4] = {0.f, 0.f, 0.f, 0.f};
+    if (I.in) {
+        /* interior: the stencil without the tile-edge tests, two pixels per
+         * instruction (the same operations in the same order per pixel) */
 #pragma unroll
-    for (int j = 0; j < kItemVx; ++j) {
-        const int c = I.c0 + j;
-        if (c >= nc) {
-            pn[j] = 0.f;
-            continue;
+        for (int j = 0; j < kItemVx; j += 2) {
+            const float2 xa = pf2(pn[j], pn[j + 1]);
+            const float2 xl = pf2(j == 0 ? lf : pn[j - 1], pn[j]);
+            const float2 xr = pf2(pn[j + 1], j + 2 == kItemVx ? rt : pn[j + 2]);
+            const float2 wl = pf2(j == 0 ? wlf : wrt[j - 1], wrt[j]);
+            float2 y = __fmul2_rn(pf2(kLapEpsF, kLapEpsF), xa);
+            y = __ffma2_rn(pf2(wdn[j], wdn[j + 1]), psub(xa, pf2(dn[j], dn[j + 1])), y);
+            y = __ffma2_rn(pf2(wup[j], wup[j + 1]), psub(xa, pf2(up[j], up[j + 1])), y);
+            y = __ffma2_rn(pf2(wrt[j], wrt[j + 1]), psub(xa, xr), y);
+            y = __ffma2_rn(wl, psub(xa, xl), y);
+            const float2 m = __fmul2_rn(y, pf2(rd[j], rd[j + 1]));
+            qv[j] = y.x; qv[j + 1] = y.y;
+            mq[j] = m.x; mq[j + 1] = m.y;
         }
-        const float xl = j == 0 ? lf : pn[j - 1];
-        const float xr = j == kItemVx - 1 ? rt : pn[j + 1];
-        const float wl = j == 0 ? wlf : wrt[j - 1];
-        const float xa = pn[j];
-        float y = __fmul_rn(kLapEpsF, xa);
-        if (r < nr - 1) y = __fmaf_rn(wdn[j], __fsub_rn(xa, dn[j]), y);
-        if (r > 0)      y = __fmaf_rn(wup[j], __fsub_rn(xa, up[j]), y);
-        if (c < nc - 1) y = __fmaf_rn(wrt[j], __fsub_rn(xa, xr), y);
-        if (c > 0)      y = __fmaf_rn(wl, __fsub_rn(xa, xl), y);
-        qv[j] = y;
-        mq[j] = __fmul_rn(y, rd[j]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < kItemVx; ++j) {
+            const int c = I.c0 + j;
+            if (c >= nc) {
+                pn[j] = 0.f;
+                continue;
+            }
+            const float xl = j == 0 ? lf : pn[j - 1];
+            const float xr = j == kItemVx - 1 ? rt : pn[j + 1];
+            const float wl = j == 0 ? wlf : wrt[j - 1];
+            const float xa = pn[j];
+            float y = __fmul_rn(kLapEpsF, xa);
+            if (r < nr - 1) y = __fmaf_rn(wdn[j], __fsub_rn(xa, dn[j]), y);
+            if (r > 0)      y = __fmaf_rn(wup[j], __fsub_rn(xa, up[j]), y);
+            if (c < nc - 1) y = __fmaf_rn(wrt[j], __fsub_rn(xa, xr), y);
+            if (c > 0)      y = __fmaf_rn(wl, __fsub_rn(xa, xl), y);
+            qv[j] = y;
+            mq[j] = __fmul_rn(y, rd[j]);
+        }
     }
-    acc[1] = dot4_df(pn, qv);
-    acc[2] = dot4_df(zn, qv);
+    dot4_df2(pn, qv, zn, qv, acc[1], acc[2]);
     acc[3] = dot4_df(qv, mq);
     st4(pnew_all + I.o, pn);
     st4(qnew_all + I.o, qv);
@@ -930,7 +994,7 @@ __device__ void phase_fold(const TileDesc &T, int li, const SolverPlanes &P, con
                            bool with_update, double alpha)
 {
     ItemXY q = item_xy(T, li);
-    if (threadIdx.x >= kItemThreads || q.r >= T.nr || q.c0 >= T.nc) return;
+    if (q.r >= T.nr || q.c0 >= T.nc) return;
     const size_t o = T.pix + (size_t)q.r * T.pitch + q.c0;
     float dxv[4], pv[4];
     double xv[4];
@@ -954,7 +1018,7 @@ template <typename V>
 __device__ void phase_rw(const TileDesc &T, int li, const SolverPlanes &P, float delta)
 {
     ItemXY q = item_xy(T, li);
-    if (threadIdx.x >= kItemThreads || q.r >= T.nr || q.c0 >= T.nc) return;
+    if (q.r >= T.nr || q.c0 >= T.nc) return;
     const double *x = P.x + T.pix;
     const double dd = (double)delta * (double)delta;
     const int r = q.r, nr = T.nr, nc = T.nc, pitch = T.pitch, pp = T.ph_pitch;
@@ -994,7 +1058,7 @@ template <typename V>
 __device__ void phase_final(const TileDesc &T, int li, const SolverPlanes &P)
 {
     ItemXY q = item_xy(T, li);
-    if (threadIdx.x >= kItemThreads || q.r >= T.nr || q.c0 >= T.nc) return;
+    if (q.r >= T.nr || q.c0 >= T.nc) return;
     const double *x = P.x + T.pix;
     double off = (double)__ldg(T.ph) - ldc(x);
     size_t prow = (size_t)q.r * T.pitch;
@@ -1250,26 +1314,14 @@ __device__ void run_pass(const SliceCtl &sc, const TileDesc *gt, const TileState
     __syncthreads();
 }
 
-/* The mixed pass runs warp-specialised: the block's last warp is the
- * producer (one lane issues every item's TMA boxes into the NS-stage ring,
- * waiting on the stage's "empty" barrier before refilling it), the other
- * kItemThreads threads consume items in the same order (wait on the stage's
- * "full" barrier, compute, arrive on "empty").  The consumers synchronise
- * among themselves once per item, with a named barrier between the two
- * halves of an item (the fold writes Pn, the stencil reads neighbours'
- * values); Pn and the warp partials alternate between two buffers by item
- * parity.  The cross-warp sum of item k's partials and their store run in
- * warp 0 after the barrier of item k+1, when every warp has finished item
- * k, so no second barrier per item is needed.  kk counts the ring's items
- * over the whole launch (stage = kk mod NS, use = kk / NS), identically in
- * every thread.  Tile totals of the pass are formed at its end, for every
- * tile of the block's slice. */
-constexpr int kConsumerBar = 1;
-__device__ __forceinline__ void consumer_sync()
-{
-    asm volatile("bar.sync %0, %1;" ::"n"(kConsumerBar), "n"(kItemThreads) : "memory");
-}
-
+/* The mixed pass over this block's slice, staged like run_pass but with one
+ * block barrier per item.  Pn and the warp partials alternate between two
+ * buffers by item parity.  After the barrier of item k (between its two
+ * halves), every thread has finished item k-1, so then warp 0 forms and
+ * stores item k-1's partials (the cross-warp sum) and thread 0 refills item
+ * k-1's stage with item k-1+NS: the boxes of the next NS-1 items are in
+ * flight while item k computes.  Tile totals of the pass are formed at its
+ * end, for every tile of the block's slice. */
 /* cross-warp sum (fixed tree, the same as block_sum4_item's warp-0 stage) of
  * one item's warp partials, stored as the item's partials */
 __device__ __forceinline__ void store_item4(const double (*red)[8], double *part, int nitems,
@@ -1290,71 +1342,68 @@ __device__ void run_pass_s(const SliceCtl &sc, const TileDesc *gt, const TileSta
                            bool fresh, float *pnew, float *rnew, float *qnew, float *dx,
                            double *part, double *tot, unsigned *cnt, double *sw,
                            double (*red)[kNComp][8], double *s_bcast, int *s_flag, float *Pn2,
-                           char *stages, uint64_t *full, uint64_t *empty, uint32_t &kk,
-                           SolverCtl *ctl, long long timeout_ns)
+                           char *stages, uint64_t *bars, uint32_t &parity, SolverCtl *ctl,
+                           long long timeout_ns)
 {
     constexpr size_t SB = stage_bytes<float>();
     constexpr size_t PNE = pn_bytes<float>() / sizeof(float);
+    if (sc.s0 >= sc.s1) return;
+    Cursor ci = cursor_active(Cursor{sc.s0, sc.t0}, sc, gt, st, ntiles);
+    if (ci.p >= sc.s1) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint32_t nit = 0;
-    if (sc.s0 < sc.s1) {
-        for (Cursor c = cursor_active(Cursor{sc.s0, sc.t0}, sc, gt, st, ntiles); c.p < sc.s1;
-             c = cursor_active(Cursor{c.p + 1, c.t}, sc, gt, st, ntiles))
-            ++nit;
+    Cursor cc = ci;
+    if (threadIdx.x == 0) {
+        fence_async_global();
+        fence_async_smem();
     }
-    if (nit > 0) {
-        if (warp == kItemThreads / 32) {
-            /* producer */
-            if (lane == 0) {
-                fence_async_global();
-                uint32_t k = kk;
-                for (Cursor c = cursor_active(Cursor{sc.s0, sc.t0}, sc, gt, st, ntiles);
-                     c.p < sc.s1; c = cursor_active(Cursor{c.p + 1, c.t}, sc, gt, st, ntiles), ++k) {
-                    const uint32_t s = k % NS, use = k / NS;
-                    if (use > 0) mbar_wait(empty + s, (use - 1) & 1u, ctl, timeout_ns);
+    for (int k = 0; k < NS && ci.p < sc.s1; ++k) {
+        if (threadIdx.x == 0)
+            issue_s(stile(sc, gt, ci.t), ci.p - sc.pre[ci.t], M, zsel, ksel, first, fresh,
+                    stages + k * SB, bars + k);
+        ci = cursor_active(Cursor{ci.p + 1, ci.t}, sc, gt, st, ntiles);
+    }
+    int k = 0, prev = -1;   /* item number in the pass; partial index of item k-1 */
+    while (cc.p < sc.s1) {
+        const int s = k % NS;
+        mbar_wait(bars + s, (parity >> s) & 1u, ctl, timeout_ns);
+        parity ^= 1u << s;
+        const TileDesc &T = stile(sc, gt, cc.t);
+        const int li = cc.p - sc.pre[cc.t];
+        const ItemS I = item_s(T, li, stages + s * SB);
+        float *Pn = Pn2 + (k & 1) * PNE;
+        double acc[kNComp] = {0.0, 0.0, 0.0, 0.0};
+        float zn[4] = {0.f, 0.f, 0.f, 0.f}, rd[4] = {0.f, 0.f, 0.f, 0.f};
+        compute_s1(T, I, rnew, dx, first, fresh, (float)salpha(sc, st, cc.t),
+                   (float)sbeta(sc, st, cc.t), Pn, zn, rd, acc);
+        __syncthreads();
+        if (prev >= 0) {
+            if (warp == 0) store_item4(red[(k - 1) & 1], part, nitems, prev);
+            if (ci.p < sc.s1) {
+                if (threadIdx.x == 0) {
+                    const int sp = (k - 1) % NS;
                     fence_async_smem();
-                    issue_s(stile(sc, gt, c.t), c.p - sc.pre[c.t], M, zsel, ksel, first, fresh,
-                            stages + s * SB, full + s);
+                    issue_s(stile(sc, gt, ci.t), ci.p - sc.pre[ci.t], M, zsel, ksel, first,
+                            fresh, stages + sp * SB, bars + sp);
                 }
+                ci = cursor_active(Cursor{ci.p + 1, ci.t}, sc, gt, st, ntiles);
             }
-        } else {
-            /* consumers */
-            uint32_t k = kk;
-            int prev = -1;   /* partial index of the previous item */
-            for (Cursor c = cursor_active(Cursor{sc.s0, sc.t0}, sc, gt, st, ntiles); c.p < sc.s1;
-                 c = cursor_active(Cursor{c.p + 1, c.t}, sc, gt, st, ntiles), ++k) {
-                const uint32_t s = k % NS;
-                mbar_wait(full + s, (k / NS) & 1u, ctl, timeout_ns);
-                const TileDesc &T = stile(sc, gt, c.t);
-                const int li = c.p - sc.pre[c.t];
-                const ItemS I = item_s(T, li, stages + s * SB);
-                float *Pn = Pn2 + (k & 1u) * PNE;
-                double acc[kNComp] = {0.0, 0.0, 0.0, 0.0};
-                float zn[4] = {0.f, 0.f, 0.f, 0.f}, rd[4] = {0.f, 0.f, 0.f, 0.f};
-                compute_s1(T, I, rnew, dx, first, fresh, (float)salpha(sc, st, c.t),
-                           (float)sbeta(sc, st, c.t), Pn, zn, rd, acc);
-                consumer_sync();
-                if (warp == 0 && prev >= 0) store_item4(red[(k - 1) & 1u], part, nitems, prev);
-                compute_s2(T, I, pnew, qnew, Pn, zn, rd, acc);
-#pragma unroll
-                for (int cc = 0; cc < kNComp; ++cc)
-                    for (int off = 16; off > 0; off >>= 1)
-                        acc[cc] += __shfl_down_sync(0xffffffffu, acc[cc], off);
-                if (lane == 0) {
-#pragma unroll
-                    for (int cc = 0; cc < kNComp; ++cc) red[k & 1u][cc][warp] = acc[cc];
-                }
-                __syncwarp();
-                if (lane == 0) mbar_arrive(empty + s);
-                prev = T.item0 + li;
-            }
-            consumer_sync();
-            if (warp == 0) store_item4(red[(k - 1) & 1u], part, nitems, prev);
         }
+        compute_s2(T, I, pnew, qnew, Pn, zn, rd, acc);
+#pragma unroll
+        for (int c = 0; c < kNComp; ++c)
+            for (int off = 16; off > 0; off >>= 1)
+                acc[c] += __shfl_down_sync(0xffffffffu, acc[c], off);
+        if (lane == 0) {
+#pragma unroll
+            for (int c = 0; c < kNComp; ++c) red[k & 1][c][warp] = acc[c];
+        }
+        prev = T.item0 + li;
+        ++k;
+        cc = cursor_active(Cursor{cc.p + 1, cc.t}, sc, gt, st, ntiles);
     }
-    kk += nit;
     __syncthreads();
-    if (nit == 0) return;
+    if (warp == 0) store_item4(red[(k - 1) & 1], part, nitems, prev);
+    __syncthreads();
     /* the block's partials of every active tile of its slice are stored */
     for (int t = sc.t0; t <= sc.t1; ++t) {
         if (sc.pre[t + 1] == sc.pre[t] || !sactive(sc, st, t)) continue;
@@ -1432,7 +1481,7 @@ __device__ __forceinline__ void carry_inactive(const TileState *from, TileState 
  * side, optional warm start, no anchoring); a separate instantiation so the
  * main path's register allocation does not carry its extra inputs */
 template <typename V, bool WLS, int NS, int MINB>
-__global__ void __launch_bounds__(solve_threads<V>()) __maxnreg__((solve_regs<V, MINB>()))
+__global__ void __launch_bounds__(kItemThreads, MINB)
     k_solve(const TileDesc *__restrict__ tiles, const int *__restrict__ item_tile, int nitems,
             int ntiles, SolverPlanes P, TileState *st, double *part, SolverCtl *ctl,
             SolveParams sp, long long timeout_ns, const __grid_constant__ SolveMaps M)
@@ -1442,7 +1491,7 @@ __global__ void __launch_bounds__(solve_threads<V>()) __maxnreg__((solve_regs<V,
     __shared__ double red[2][kNComp][8];   /* mixed: warp partials by item parity */
     __shared__ double s_bcast;
     __shared__ int s_flag;
-    __shared__ __align__(8) uint64_t bars[2 * NS];   /* ring: full [0, NS), empty [NS, 2 NS) */
+    __shared__ __align__(8) uint64_t bars[NS];
     __shared__ SliceCtl sc;
     char *dsm = (char *)(((uintptr_t)dsm_raw + 127) & ~(uintptr_t)127);
     constexpr bool mixed = sizeof(V) == 4;
@@ -1459,14 +1508,10 @@ __global__ void __launch_bounds__(solve_threads<V>()) __maxnreg__((solve_regs<V,
     /* z buffers: the first is written by the assembly; mixed mode
      * double-buffers z in the r plane (r = z diag is not stored) */
     V *zb[2] = {(V *)P.z, (V *)P.r};
-    uint32_t parity = 0u;   /* FP64 ring: phase bit per stage */
-    uint32_t kk = 0u;       /* mixed ring: items so far */
+    uint32_t parity = 0u;   /* phase bit per stage of the ring */
     (void)item_tile;
     if (threadIdx.x == 0) {
-        for (int k = 0; k < NS; ++k) {
-            mbar_init(&bars[k]);
-            mbar_init_n(&bars[NS + k], kItemThreads / 32);
-        }
+        for (int k = 0; k < NS; ++k) mbar_init(&bars[k]);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -1667,8 +1712,7 @@ __global__ void __launch_bounds__(solve_threads<V>()) __maxnreg__((solve_regs<V,
                 run_pass_s<NS>(sc, tiles, st + (size_t)cur * ntiles, ntiles, nitems, M, zsel, k & 1,
                            k == 0, fresh, (float *)pb[(k + 1) & 1], (float *)zb[zsel ^ 1],
                            qb[(k + 1) & 1], P.dx, pbuf[pc & 1], tbuf[pc & 1], tick, sw, red,
-                           &s_bcast, &s_flag, (float *)Pn, dsm, bars, bars + NS, kk, ctl,
-                           timeout_ns);
+                           &s_bcast, &s_flag, (float *)Pn, dsm, bars, parity, ctl, timeout_ns);
                 ++pc;
                 if (!fresh) zsel ^= 1;
                 prev_fresh = fresh;
@@ -1800,14 +1844,14 @@ static int launch_solve_shape(const TileDesc *tiles, const int *item_tile, int n
     auto kern = k_solve<V, WLS, NS, MINB>;
     CUPHU_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)smem));
-    constexpr int BT = solve_threads<V>();
-    CUPHU_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BT, smem));
+    CUPHU_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kItemThreads,
+                                                                 smem));
     if (per_sm < 1) return fail(CUPHU_ERR_CUDA, "solver kernel cannot be resident");
     per_sm = std::min(per_sm, MINB);
     int grid = std::min(nsm * per_sm, std::max(nitems, 1));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(BT);
+    cfg.blockDim = dim3(kItemThreads);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
@@ -1837,7 +1881,7 @@ static int launch_solve_kernel(const TileDesc *tiles, const int *item_tile, int 
     if constexpr (sizeof(V) == 4) {
         switch (v) {
         case 1: CUPHU_SOLVE_SHAPE(2, 2);
-        case 2: CUPHU_SOLVE_SHAPE(5, 1);
+        case 2: CUPHU_SOLVE_SHAPE(6, 1);
         default: CUPHU_SOLVE_SHAPE(3, 2);
         }
     } else {
@@ -1853,7 +1897,7 @@ int solve_shape_count(bool fp64) { return fp64 ? 2 : 3; }
 
 void solve_shape_of(bool fp64, int v, int *stages, int *blocks_per_sm)
 {
-    static const int mixed[3][2] = {{3, 2}, {2, 2}, {5, 1}};
+    static const int mixed[3][2] = {{3, 2}, {2, 2}, {6, 1}};
     static const int f64[2][2] = {{2, 2}, {3, 1}};
     const int(*t)[2] = fp64 ? f64 : mixed;
     const int n = solve_shape_count(fp64);

@@ -270,7 +270,7 @@ int cuphu_laplace_solve_device(const void *d_costs, int cost_stride_shorts,
  * Times, on the caller's scene (host pointers, uploaded here), the cost
  * kernel at 3 and 4 blocks per SM and the persistent solver in each of its
  * launch shapes (stages of the per-block shared-memory ring x resident
- * blocks per SM; mixed precision: 3x2, 2x2, 5x1) with a 20-iteration probe
+ * blocks per SM; mixed precision: 3x2, 2x2, 6x1) with a 20-iteration probe
  * of the given tiling, and stores the fastest choice per device and
  * job-size class (floor(log2) of the arc or work-item count) for all later
  * calls.  choices (optional, int[2]) receives {cost variant 0|1, solver

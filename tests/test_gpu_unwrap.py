@@ -149,7 +149,7 @@ def test_autotune_keeps_results(torch_cuda):
                                       n_irls=2)
     ch = cuphu_b200.autotune(ig, g, 5.0, cost="defo", ntiles=(2, 2), tile_overlap=(16, 16))
     assert ch["cost_blocks_per_sm"] in (3, 4) and ch["solver_blocks_per_sm"] in (1, 2)
-    assert ch["solver_stages"] in (2, 3, 5)
+    assert ch["solver_stages"] in (2, 3, 6)
     u, c, _ = device_unwrap(torch_cuda, ph, g, 5.0, (2, 2), (16, 16), precision=1, n_irls=2)
     assert np.array_equal(u.view(np.int32), base_u.view(np.int32))
     assert np.array_equal(c, base_c)
