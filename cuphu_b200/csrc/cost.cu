@@ -748,43 +748,42 @@ __global__ void __launch_bounds__(256, MINB) k_costs7(const float *__restrict__ 
     for (int half = 0; half < 2; ++half) {
     const int rs = rs0 + half * 4;
     if (r0 + rs >= dr) break;
-    float2 w[10];
-#pragma unroll
-    for (int q = 0; q < 10; ++q) w[q] = tp[(rs + q) * kC7H + j];
-    /* the strip's coherence: rows rs..rs+4 (FAM 0) or columns ac, ac+1 of
-     * rows rs..rs+3 (FAM 1), loaded together */
-    float cv[2][5], cw[2][4];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const int ac = c0 + j + h * kC7H;
-#pragma unroll
-        for (int q = 0; q < 5; ++q) {
-            const int rr = r0 + rs + q;
-            cv[h][q] = 0.0f;
-            if (q < 4) cw[h][q] = 0.0f;
-            if (tma) {
-                /* staged window: row rs+q, column j+32h (+1); zero outside the array */
-                const float *cp = S.cor + (rs + q) * kC7CorW + j + h * kC7H;
-                if (FAM == 0) cv[h][q] = cp[0];
-                else if (q < 4) { cv[h][q] = cp[0]; cw[h][q] = cp[1]; }
-            } else if (FAM == 0) {
-                if (ac < dc && rr < nrow) cv[h][q] = __ldg(corr + (size_t)rr * ncol + ac);
-            } else if (q < 4 && ac < dc && rr < nrow) {
-                cv[h][q] = __ldg(corr + (size_t)rr * ncol + ac);
-                cw[h][q] = __ldg(corr + (size_t)rr * ncol + ac + 1);
-            }
-            cv[h][q] = cor_fast(cv[h][q]);
-            if (q < 4) cw[h][q] = cor_fast(cw[h][q]);
+    /* a rolling window of the row sums and of the coherence: each row of
+     * the strip loads one new row sum and its coherence (fewer live
+     * registers than loading the whole strip up front) */
+    auto cor_at = [&](int q, int h, int dcol) -> float {
+        const int ac = c0 + j + h * kC7H, rr = r0 + rs + q;
+        float v = 0.0f;
+        if (tma) {
+            /* staged window: row rs+q, column j+32h (+1); zero outside the array */
+            v = S.cor[(rs + q) * kC7CorW + j + h * kC7H + dcol];
+        } else if (ac < dc && rr < nrow) {
+            v = __ldg(corr + (size_t)rr * ncol + ac + dcol);
         }
-    }
+        return cor_fast(v);
+    };
+    float2 w[7];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) w[q] = tp[(rs + q) * kC7H + j];
+    float2 cnext = FAM == 0 ? f2(cor_at(0, 0, 0), cor_at(0, 1, 0)) : f2(0.0f, 0.0f);
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
         const int ar = r0 + rs + m;
         if (ar >= dr) break;
-        const float2 avg = boxcar7(w + m);
+        w[6] = tp[(rs + m + 6) * kC7H + j];
+        const float2 avg = boxcar7(w);
+#pragma unroll
+        for (int q = 0; q < 6; ++q) w[q] = w[q + 1];
         const float2 dps = S.dpp[(rs + m + 3) * kC7PP + j + 3];
-        const float2 ca2 = f2(cv[0][m], cv[1][m]);
-        const float2 cb2 = FAM == 0 ? f2(cv[0][m + 1], cv[1][m + 1]) : f2(cw[0][m], cw[1][m]);
+        float2 ca2, cb2;
+        if (FAM == 0) {
+            ca2 = cnext;
+            cb2 = f2(cor_at(m + 1, 0, 0), cor_at(m + 1, 1, 0));
+            cnext = cb2;
+        } else {
+            ca2 = f2(cor_at(m, 0, 0), cor_at(m, 1, 0));
+            cb2 = f2(cor_at(m, 0, 1), cor_at(m, 1, 1));
+        }
         ArcCost of[2];
         bool okf[2] = {false, false};
         if (fast) arc_fast2<DEFO>(ca2, cb2, dps, avg, k, S.lay, ntab, of[0], of[1], okf[0], okf[1]);

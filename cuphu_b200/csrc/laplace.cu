@@ -905,9 +905,12 @@ __device__ __forceinline__ void compute_s1(const TileDesc &T, const ItemS &I, fl
     }
 #pragma unroll
     for (int j = 0; j < kItemVx; ++j) Pn[I.so + j] = pn[j];
-    /* halo ring: the same update and fold, so neighbours agree bit for bit */
-    if (threadIdx.x < 2 * kItemBx + 2 * kItemBy) {
-        int h = threadIdx.x, i, jc;
+    /* halo ring: the same update and fold, so neighbours agree bit for bit;
+     * done by the last 160 threads (warps 3-7), as warps 0-3 store the
+     * previous item's partials after the barrier */
+    constexpr int kHalo = 2 * kItemBx + 2 * kItemBy;
+    if ((int)threadIdx.x >= kItemThreads - kHalo) {
+        int h = (int)threadIdx.x - (kItemThreads - kHalo), i, jc;
         if (h < kItemBx) { i = 0; jc = 4 + h; }
         else if (h < 2 * kItemBx) { i = kItemBy + 1; jc = 4 + h - kItemBx; }
         else if (h < 2 * kItemBx + kItemBy) { i = 1 + h - 2 * kItemBx; jc = 3; }
@@ -1317,23 +1320,21 @@ __device__ void run_pass(const SliceCtl &sc, const TileDesc *gt, const TileState
 /* The mixed pass over this block's slice, staged like run_pass but with one
  * block barrier per item.  Pn and the warp partials alternate between two
  * buffers by item parity.  After the barrier of item k (between its two
- * halves), every thread has finished item k-1, so then warp 0 forms and
- * stores item k-1's partials (the cross-warp sum) and thread 0 refills item
- * k-1's stage with item k-1+NS: the boxes of the next NS-1 items are in
- * flight while item k computes.  Tile totals of the pass are formed at its
+ * halves), every thread has finished item k-1, so then one thread of warp
+ * 7 refills item k-1's stage with item k-1+NS (the boxes of the next NS-1 items are in
+ * flight while item k computes) and warps 0-3 form and store item k-1's
+ * four partials (cross-warp sums, one component per warp).  Tile totals of the pass are formed at its
  * end, for every tile of the block's slice. */
-/* cross-warp sum (fixed tree, the same as block_sum4_item's warp-0 stage) of
- * one item's warp partials, stored as the item's partials */
-__device__ __forceinline__ void store_item4(const double (*red)[8], double *part, int nitems,
-                                            int item)
+/* cross-warp sum of component c of one item's eight warp partials (a fixed
+ * three-level tree), stored as the item's partial; warp c calls it */
+__device__ __forceinline__ void store_item_comp(const double (*red)[8], int c, double *part,
+                                                int nitems, int item)
 {
     const int lane = threadIdx.x & 31;
-#pragma unroll
-    for (int c = 0; c < kNComp; ++c) {
-        double x = lane < kItemThreads / 32 ? red[c][lane] : 0.0;
-        for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
-        if (lane == 0) part[(size_t)c * nitems + item] = x;
-    }
+    double x = lane < kItemThreads / 32 ? red[c][lane] : 0.0;
+    for (int off = kItemThreads / 64; off > 0; off >>= 1)
+        x += __shfl_down_sync(0xffffffffu, x, off);
+    if (lane == 0) part[(size_t)c * nitems + item] = x;
 }
 
 template <int NS>
@@ -1351,13 +1352,15 @@ __device__ void run_pass_s(const SliceCtl &sc, const TileDesc *gt, const TileSta
     Cursor ci = cursor_active(Cursor{sc.s0, sc.t0}, sc, gt, st, ntiles);
     if (ci.p >= sc.s1) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    /* the issuing thread: warp 7, whose post-barrier work is lightest */
+    const bool issuer = threadIdx.x == kItemThreads - 32;
     Cursor cc = ci;
-    if (threadIdx.x == 0) {
+    if (issuer) {
         fence_async_global();
         fence_async_smem();
     }
     for (int k = 0; k < NS && ci.p < sc.s1; ++k) {
-        if (threadIdx.x == 0)
+        if (issuer)
             issue_s(stile(sc, gt, ci.t), ci.p - sc.pre[ci.t], M, zsel, ksel, first, fresh,
                     stages + k * SB, bars + k);
         ci = cursor_active(Cursor{ci.p + 1, ci.t}, sc, gt, st, ntiles);
@@ -1377,9 +1380,8 @@ __device__ void run_pass_s(const SliceCtl &sc, const TileDesc *gt, const TileSta
                    (float)sbeta(sc, st, cc.t), Pn, zn, rd, acc);
         __syncthreads();
         if (prev >= 0) {
-            if (warp == 0) store_item4(red[(k - 1) & 1], part, nitems, prev);
             if (ci.p < sc.s1) {
-                if (threadIdx.x == 0) {
+                if (issuer) {
                     const int sp = (k - 1) % NS;
                     fence_async_smem();
                     issue_s(stile(sc, gt, ci.t), ci.p - sc.pre[ci.t], M, zsel, ksel, first,
@@ -1387,6 +1389,7 @@ __device__ void run_pass_s(const SliceCtl &sc, const TileDesc *gt, const TileSta
                 }
                 ci = cursor_active(Cursor{ci.p + 1, ci.t}, sc, gt, st, ntiles);
             }
+            if (warp < kNComp) store_item_comp(red[(k - 1) & 1], warp, part, nitems, prev);
         }
         compute_s2(T, I, pnew, qnew, Pn, zn, rd, acc);
 #pragma unroll
@@ -1402,7 +1405,7 @@ __device__ void run_pass_s(const SliceCtl &sc, const TileDesc *gt, const TileSta
         cc = cursor_active(Cursor{cc.p + 1, cc.t}, sc, gt, st, ntiles);
     }
     __syncthreads();
-    if (warp == 0) store_item4(red[(k - 1) & 1], part, nitems, prev);
+    if (warp < kNComp) store_item_comp(red[(k - 1) & 1], warp, part, nitems, prev);
     __syncthreads();
     /* the block's partials of every active tile of its slice are stored */
     for (int t = sc.t0; t <= sc.t1; ++t) {
