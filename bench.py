@@ -41,9 +41,11 @@ FALLBACK_HBM = 6650.0
 METRIC = "Mpix/s unwrapped at 8192^2 (mixed-precision Laplace PCG)"
 
 
-# measured k_solve DRAM bytes (mixed precision), see the roofline block
-TRAFFIC_PER_PX_ITER = 50.3
-TRAFFIC_PER_PASS_PX = 65.0
+# measured k_solve DRAM bytes (mixed precision), see the roofline block:
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of the 4096^2 case at 20
+# and 40 PCG iterations (one pass): 17.69 and 33.65 GB
+TRAFFIC_PER_PX_ITER = 43.4
+TRAFFIC_PER_PASS_PX = 94.3
 
 
 def hbm_peak():

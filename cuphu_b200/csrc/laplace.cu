@@ -24,17 +24,17 @@
  *    the update pass moves x, r and z.
  *  - Mixed mode runs ONE pass and ONE grid barrier per iteration (a
  *    single-synchronisation form of the same Jacobi-PCG).  The solution is an
- *    FP64 base x plus an FP32 increment dx; z, p, q are FP32 (r = z diag is
- *    not stored) and both z and q are double-buffered like p.  Each pass
- *    applies the previous iteration's update (dx += alpha p_old,
- *    z = (z diag - alpha q) / diag), folds p = z + beta p_old, own pixels and
- *    halo alike, and computes q = A p, recomputing diag from the staged arc
- *    weights; it reduces r.z, p.q, z.q and q.(q/diag) in FP64 in one tree.
- *    alpha and the stop test use the true r.z of the pass; beta uses the
- *    one-step recurrence r.z' = r.z - 2 alpha z.q + alpha^2 q.(q/diag)
- *    anchored at that true value.  Every `replace_every` iterations the
- *    increment is folded into x and the recursive residual is replaced by
- *    the true residual b - A x (FP64).
+ *    FP64 base x plus an FP32 increment dx; r, p, q are FP32 and each is
+ *    double-buffered.  Each pass applies the previous iteration's update
+ *    (dx += alpha p_old, r = r - alpha q), forms z = M^-1 r (M^-1 the
+ *    hardware reciprocal of an FP32 Jacobi diagonal summed from the staged
+ *    arc weights), folds p = z + beta p_old, own pixels and halo alike, and
+ *    computes q = A p; it reduces r.z, p.q, z.q and q.M^-1 q with FP64
+ *    accuracy in one tree.  alpha and the stop test use the true r.z of the
+ *    pass; beta uses the one-step recurrence
+ *    r.z' = r.z - 2 alpha z.q + alpha^2 q.M^-1 q anchored at that true value.
+ *    Every `replace_every` iterations the increment is folded into x and the
+ *    recursive residual is replaced by the true residual b - A x (FP64).
  */
 #include "kernels.cuh"
 
@@ -785,16 +785,16 @@ __device__ __forceinline__ void issue_s(const TileDesc &T, int li, const SolveMa
     if (!fresh) tma_load_2d(stage + StageS::oDX, &M.xB, c0b, y, bar);
 }
 
-/* One item of the mixed pass, in two halves around the consumer barrier.
+/* One item of the mixed pass, in two halves around the block barrier.
  * FP32 arithmetic for the vector updates and the stencil (IEEE
  * round-to-nearest per operation), FP64-accurate dots (dot4_df per thread):
  * acc[0] r.z of the updated residual (when not fresh), acc[1] p.q, acc[2]
  * z.q, acc[3] q.(M^-1 q).  The residual plane holds r; z = M^-1 r is formed
  * on the fly with M^-1 = rcp_pre(diag32) of the staged weights.
  * compute_s1: the previous iteration's update and the fold p' = z' + beta
- * p_old of the own pixels and the halo ring, into Pn; only z' and M^-1 of
+ * p_old of the own pixels and the halo ring, into Pn; r', z' and M^-1 of
  * the own pixels stay in registers for compute_s2, which computes q = A p'
- * from Pn and the staged weights. */
+ * from Pn and the staged weights, and all four dots (two at a time). */
 struct ItemS {
     const float *R, *Q, *PO, *WR, *WD, *DX;
     int r0b, c0b, ty, tx, r, c0, so, sd;
@@ -832,7 +832,7 @@ __device__ __forceinline__ ItemS item_s(const TileDesc &T, int li, const char *s
 __device__ __forceinline__ void compute_s1(const TileDesc &T, const ItemS &I, float *rnew_all,
                                            float *dx_all, bool first, bool fresh, float alphaf,
                                            float betaf, float *Pn, float zn[4], float rd[4],
-                                           double acc[kNComp])
+                                           float rv[4])
 {
     const int nr = T.nr, nc = T.nc;
     float pn[4] = {0.f, 0.f, 0.f, 0.f};
@@ -842,7 +842,7 @@ __device__ __forceinline__ void compute_s1(const TileDesc &T, const ItemS &I, fl
         sld4(I.WD + I.sd - kSegW, wup);
         sld4(I.WR + I.so, wrt);
         const float wlf = I.WR[I.so - 1];
-        float rv[4], qv[4] = {0.f, 0.f, 0.f, 0.f}, pv[4] = {0.f, 0.f, 0.f, 0.f};
+        float qv[4] = {0.f, 0.f, 0.f, 0.f}, pv[4] = {0.f, 0.f, 0.f, 0.f};
         float dxv[4] = {0.f, 0.f, 0.f, 0.f};
         sld4(I.R + I.so, rv);
         if (!fresh) {
@@ -898,7 +898,6 @@ __device__ __forceinline__ void compute_s1(const TileDesc &T, const ItemS &I, fl
             }
         }
         if (!fresh) {
-            acc[0] = dot4_df(rv, zn);
             st4(dx_all + I.o, dxv);
             st4(rnew_all + I.o, rv);
         }
@@ -931,7 +930,8 @@ __device__ __forceinline__ void compute_s1(const TileDesc &T, const ItemS &I, fl
 
 __device__ __forceinline__ void compute_s2(const TileDesc &T, const ItemS &I, float *pnew_all,
                                            float *qnew_all, const float *Pn, const float zn[4],
-                                           const float rd[4], double acc[kNComp])
+                                           const float rd[4], const float rv[4], bool fresh,
+                                           double acc[kNComp])
 {
     if (!I.own) return;
     const int nr = T.nr, nc = T.nc, r = I.r, so = I.so;
@@ -985,7 +985,8 @@ __device__ __forceinline__ void compute_s2(const TileDesc &T, const ItemS &I, fl
         }
     }
     dot4_df2(pn, qv, zn, qv, acc[1], acc[2]);
-    acc[3] = dot4_df(qv, mq);
+    if (fresh) acc[3] = dot4_df(qv, mq);
+    else dot4_df2(qv, mq, rv, zn, acc[3], acc[0]);
     st4(pnew_all + I.o, pn);
     st4(qnew_all + I.o, qv);
 }
@@ -1376,8 +1377,9 @@ __device__ void run_pass_s(const SliceCtl &sc, const TileDesc *gt, const TileSta
         float *Pn = Pn2 + (k & 1) * PNE;
         double acc[kNComp] = {0.0, 0.0, 0.0, 0.0};
         float zn[4] = {0.f, 0.f, 0.f, 0.f}, rd[4] = {0.f, 0.f, 0.f, 0.f};
+        float rv[4] = {0.f, 0.f, 0.f, 0.f};
         compute_s1(T, I, rnew, dx, first, fresh, (float)salpha(sc, st, cc.t),
-                   (float)sbeta(sc, st, cc.t), Pn, zn, rd, acc);
+                   (float)sbeta(sc, st, cc.t), Pn, zn, rd, rv);
         __syncthreads();
         if (prev >= 0) {
             if (ci.p < sc.s1) {
@@ -1391,14 +1393,24 @@ __device__ void run_pass_s(const SliceCtl &sc, const TileDesc *gt, const TileSta
             }
             if (warp < kNComp) store_item_comp(red[(k - 1) & 1], warp, part, nitems, prev);
         }
-        compute_s2(T, I, pnew, qnew, Pn, zn, rd, acc);
-#pragma unroll
-        for (int c = 0; c < kNComp; ++c)
-            for (int off = 16; off > 0; off >>= 1)
-                acc[c] += __shfl_down_sync(0xffffffffu, acc[c], off);
-        if (lane == 0) {
-#pragma unroll
-            for (int c = 0; c < kNComp; ++c) red[k & 1][c][warp] = acc[c];
+        compute_s2(T, I, pnew, qnew, Pn, zn, rd, rv, fresh, acc);
+        {
+            /* warp sums of the four components by a reduce-scatter tree:
+             * after the xor-16 and xor-8 steps each lane holds one
+             * component (lanes 8c..8c+7 component c), then three plain
+             * levels; lane 8c ends with the warp's component c */
+            const bool hi16 = lane & 16, hi8 = lane & 8;
+            const double s0 = hi16 ? acc[0] : acc[2], s1v = hi16 ? acc[1] : acc[3];
+            const double r0 = __shfl_xor_sync(0xffffffffu, s0, 16);
+            const double r1 = __shfl_xor_sync(0xffffffffu, s1v, 16);
+            const double k0 = (hi16 ? acc[2] : acc[0]) + r0;
+            const double k1 = (hi16 ? acc[3] : acc[1]) + r1;
+            const double r2 = __shfl_xor_sync(0xffffffffu, hi8 ? k0 : k1, 8);
+            double v = (hi8 ? k1 : k0) + r2;
+            v += __shfl_xor_sync(0xffffffffu, v, 4);
+            v += __shfl_xor_sync(0xffffffffu, v, 2);
+            v += __shfl_xor_sync(0xffffffffu, v, 1);
+            if ((lane & 7) == 0) red[k & 1][lane >> 3][warp] = v;
         }
         prev = T.item0 + li;
         ++k;
@@ -1508,8 +1520,8 @@ __global__ void __launch_bounds__(kItemThreads, MINB)
     unsigned *tick = reinterpret_cast<unsigned *>(part + 2 * (size_t)kNComp * nitems +
                                                   2 * (size_t)kNComp * ntiles);
     V *Pn = (V *)(dsm + NS * stage_bytes<V>());
-    /* z buffers: the first is written by the assembly; mixed mode
-     * double-buffers z in the r plane (r = z diag is not stored) */
+    /* FP64: z (written by the assembly); mixed: the residual r, double-
+     * buffered in the z and r planes */
     V *zb[2] = {(V *)P.z, (V *)P.r};
     uint32_t parity = 0u;   /* phase bit per stage of the ring */
     (void)item_tile;
