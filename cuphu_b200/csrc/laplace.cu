@@ -158,6 +158,27 @@ __device__ void seg_done(const TileDesc &T, int t, int nseg, const double *part,
 
 /* seg_done for the kNComp-component partials of the mixed pass: component c
  * of item i at part[c * nitems + i], of tile t at tot[c * ntiles + t] */
+/* warp sums of four values by a reduce-scatter tree: after the xor-16 and
+ * xor-8 steps each lane holds one component (lanes 8c..8c+7 component c),
+ * then three plain levels; every lane of group c returns the warp's sum of
+ * component c (the same value in all eight lanes) */
+__device__ __forceinline__ double warp_scatter4(const double a[kNComp])
+{
+    static_assert(kNComp == 4, "four components");
+    const int lane = threadIdx.x & 31;
+    const bool hi16 = lane & 16, hi8 = lane & 8;
+    const double r0 = __shfl_xor_sync(0xffffffffu, hi16 ? a[0] : a[2], 16);
+    const double r1 = __shfl_xor_sync(0xffffffffu, hi16 ? a[1] : a[3], 16);
+    const double k0 = (hi16 ? a[2] : a[0]) + r0;
+    const double k1 = (hi16 ? a[3] : a[1]) + r1;
+    const double r2 = __shfl_xor_sync(0xffffffffu, hi8 ? k0 : k1, 8);
+    double v = (hi8 ? k1 : k0) + r2;
+    v += __shfl_xor_sync(0xffffffffu, v, 4);
+    v += __shfl_xor_sync(0xffffffffu, v, 2);
+    v += __shfl_xor_sync(0xffffffffu, v, 1);
+    return v;
+}
+
 __device__ void seg_done4(const TileDesc &T, int t, int nseg, const double *part, int nitems,
                           double *tot, int ntiles, unsigned *cnt, double *sw, double *s_bcast,
                           int *s_flag)
@@ -172,11 +193,27 @@ __device__ void seg_done4(const TileDesc &T, int t, int nseg, const double *part
     }
     __syncthreads();
     if (*s_flag) {
-        for (int c = 0; c < kNComp; ++c) {
-            double v = tile_reduce(T, part + (size_t)c * nitems, sw, s_bcast);
-            if (threadIdx.x == 0) tot[(size_t)c * ntiles + t] = v;
+        /* the four tile totals in one sweep, in a fixed order: thread j
+         * sums items j, j+256, ... per component, then the warp trees
+         * (warp_scatter4) and a three-level tree over the eight warps */
+        double a[kNComp] = {0.0, 0.0, 0.0, 0.0};
+        for (int i = threadIdx.x; i < T.nitems; i += blockDim.x)
+#pragma unroll
+            for (int c = 0; c < kNComp; ++c)
+                a[c] = a[c] + __ldcg(part + (size_t)c * nitems + T.item0 + i);
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        const double v = warp_scatter4(a);
+        if ((lane & 7) == 0) sw[(lane >> 3) * 8 + warp] = v;
+        __syncthreads();
+        if (warp == 0) {
+            double x = sw[(lane >> 3) * 8 + (lane & 7)];
+            x += __shfl_xor_sync(0xffffffffu, x, 4);
+            x += __shfl_xor_sync(0xffffffffu, x, 2);
+            x += __shfl_xor_sync(0xffffffffu, x, 1);
+            if ((lane & 7) == 0) tot[(size_t)(lane >> 3) * ntiles + t] = x;
         }
         if (threadIdx.x == 0) cnt[t] = 0u;
+        __syncthreads();
     }
 }
 
@@ -1395,21 +1432,7 @@ __device__ void run_pass_s(const SliceCtl &sc, const TileDesc *gt, const TileSta
         }
         compute_s2(T, I, pnew, qnew, Pn, zn, rd, rv, fresh, acc);
         {
-            /* warp sums of the four components by a reduce-scatter tree:
-             * after the xor-16 and xor-8 steps each lane holds one
-             * component (lanes 8c..8c+7 component c), then three plain
-             * levels; lane 8c ends with the warp's component c */
-            const bool hi16 = lane & 16, hi8 = lane & 8;
-            const double s0 = hi16 ? acc[0] : acc[2], s1v = hi16 ? acc[1] : acc[3];
-            const double r0 = __shfl_xor_sync(0xffffffffu, s0, 16);
-            const double r1 = __shfl_xor_sync(0xffffffffu, s1v, 16);
-            const double k0 = (hi16 ? acc[2] : acc[0]) + r0;
-            const double k1 = (hi16 ? acc[3] : acc[1]) + r1;
-            const double r2 = __shfl_xor_sync(0xffffffffu, hi8 ? k0 : k1, 8);
-            double v = (hi8 ? k1 : k0) + r2;
-            v += __shfl_xor_sync(0xffffffffu, v, 4);
-            v += __shfl_xor_sync(0xffffffffu, v, 2);
-            v += __shfl_xor_sync(0xffffffffu, v, 1);
+            const double v = warp_scatter4(acc);   /* lane 8c: the warp's component c */
             if ((lane & 7) == 0) red[k & 1][lane >> 3][warp] = v;
         }
         prev = T.item0 + li;
