@@ -443,16 +443,19 @@ __device__ __forceinline__ void c7_tma_2d(void *dst, const CUtensorMap *map, int
         "l"(map), "r"(x), "r"(y), "r"(c7_smem(bar))
         : "memory");
 }
-/* bounded wait for the block's TMA boxes (parity 0: one use per block) */
+/* bounded wait for the block's TMA boxes (parity 0: one use per block); a
+ * thread whose boxes have not landed may be suspended for up to 20 us per
+ * test (the suspend-time hint), so waiting warps leave the issue slots to
+ * the other blocks' computing warps */
 __device__ __forceinline__ void c7_wait(unsigned long long *bar)
 {
-    for (int i = 0; i < (1 << 24); ++i) {
+    for (int i = 0; i < (1 << 20); ++i) {
         unsigned ok;
         asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n"
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0, %2;\n"
             " selp.u32 %0, 1, 0, p;\n}"
             : "=r"(ok)
-            : "r"(c7_smem(bar))
+            : "r"(c7_smem(bar)), "r"(20000u)
             : "memory");
         if (ok) return;
     }
