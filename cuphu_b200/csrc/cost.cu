@@ -622,17 +622,19 @@ __device__ __forceinline__ void store_arc(void *costs, size_t a, const ArcCost &
         reinterpret_cast<short2 *>(costs)[a] = make_short2(o.off, o.sigsq);
 }
 
-template <bool DEFO, int FAM, int MINB>
+template <bool DEFO, int FAM, int MINB, bool TMA>
 __global__ void __launch_bounds__(256, MINB) k_costs7(const float *__restrict__ ph,
                                                    const float *__restrict__ corr,
                                                    const short *__restrict__ weights, int nrow,
                                                    int ncol, const CostConsts k,
                                                    void *__restrict__ costs_out, int nbx,
                                                    C7Global *__restrict__ gq, unsigned *gqn,
-                                                   unsigned gqcap, int tma,
+                                                   unsigned gqcap,
                                                    const __grid_constant__ CUtensorMap tm_ph,
                                                    const __grid_constant__ CUtensorMap tm_cor)
 {
+    /* TMA: the windows arrive as TMA boxes (else the threads load them) */
+    constexpr bool tma = TMA;
     extern __shared__ __align__(16) char c7raw[];
     C7Smem &S = *reinterpret_cast<C7Smem *>(
         ((uintptr_t)c7raw + 127) & ~(uintptr_t)127);
@@ -670,14 +672,20 @@ __global__ void __launch_bounds__(256, MINB) k_costs7(const float *__restrict__ 
         c7_wait(&S.bar);
     }
     if (interior && tma) {
-        /* differences from the row-major window (column c0-3+j is win[.][j+1]) */
-        for (int u = tid; u < kC7W * ND; u += blockDim.x) {
-            const int i = u / ND, j = u - (u / ND) * ND;
-            const float *w0 = S.win + i * kC7WinW + j + 1;
-            const float2 x = FAM == 0
-                                 ? sub2(f2(w0[0], w0[kC7H]), f2(w0[kC7WinW], w0[kC7WinW + kC7H]))
-                                 : sub2(f2(w0[1], w0[kC7H + 1]), f2(w0[0], w0[kC7H]));
-            S.dpp[i * kC7PP + j] = wrap2(div_2pi2(x));
+        /* differences from the row-major window (column c0-3+j is win[.][j+1]):
+         * thread (i0, j) takes rows i0, i0 + RS, ... of pair column j, so the
+         * addresses advance by constants */
+        constexpr int RS = 256 / ND;
+        if (tid < RS * ND) {
+            const int i0 = tid / ND, j = tid - i0 * ND;
+            const float *w0 = S.win + i0 * kC7WinW + j + 1;
+            float2 *dst = S.dpp + i0 * kC7PP + j;
+            for (int i = i0; i < kC7W; i += RS, w0 += RS * kC7WinW, dst += RS * kC7PP) {
+                const float2 x =
+                    FAM == 0 ? sub2(f2(w0[0], w0[kC7H]), f2(w0[kC7WinW], w0[kC7WinW + kC7H]))
+                             : sub2(f2(w0[1], w0[kC7H + 1]), f2(w0[0], w0[kC7H]));
+                *dst = wrap2(div_2pi2(x));
+            }
         }
     } else if (interior) {
         /* all of a thread's window loads in flight before the first store */
@@ -790,23 +798,19 @@ __global__ void __launch_bounds__(256, MINB) k_costs7(const float *__restrict__ 
         ArcCost of[2];
         bool okf[2] = {false, false};
         if (fast) arc_fast2<DEFO>(ca2, cb2, dps, avg, k, S.lay, ntab, of[0], of[1], okf[0], okf[1]);
+        /* arc index of the strip's column pair in this row (column j, j + 32) */
+        const size_t a0 = (FAM == 0 ? (size_t)ar * ncol : nra + (size_t)ar * (ncol - 1)) +
+                          (size_t)(c0 + j);
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int ac = c0 + j + h * kC7H;
             if (ac >= dc) continue;
             const float dpv = h ? dps.y : dps.x, avv = h ? avg.y : avg.x;
-            const size_t a = FAM == 0 ? (size_t)ar * ncol + ac
-                                      : nra + (size_t)ar * (ncol - 1) + ac;
-            const short wt = weights ? weights[a] : (short)1;
-            if (wt == 0) {
-                ArcCost o;
-                o.off = kLargeShort / 2; o.sigsq = kLargeShort;
-                o.dzmax = kLargeShort; o.laycost = 0;
-                store_arc<DEFO>(costs_out, a, o);
-            } else if (wt == 1 && okf[h]) {
-                store_arc<DEFO>(costs_out, a, of[h]);
-            } else {
-                /* the stored coherence (cor_fast changed values it rejects) */
+            const size_t a = a0 + (size_t)(h * kC7H);
+            /* an arc the fast path could not decide: queued for the exact
+             * arithmetic with the stored coherence (cor_fast changed values
+             * it rejects) */
+            auto defer = [&](short wt) {
                 const float *cp = corr + (size_t)ar * ncol + ac;
                 const float ca = sane(__ldg(cp)), cb = sane(__ldg(cp + (FAM == 0 ? ncol : 1)));
                 const int slot = atomicAdd(&S.qn, 1);
@@ -815,6 +819,23 @@ __global__ void __launch_bounds__(256, MINB) k_costs7(const float *__restrict__ 
                 } else {
                     store_arc<DEFO>(costs_out, a,
                                     arc_cost<DEFO>((double)ca, (double)cb, dpv, avv, wt, k));
+                }
+            };
+            if (!weights) {
+                /* every weight 1 */
+                if (okf[h]) store_arc<DEFO>(costs_out, a, of[h]);
+                else defer((short)1);
+            } else {
+                const short wt = weights[a];
+                if (wt == 0) {
+                    ArcCost o;
+                    o.off = kLargeShort / 2; o.sigsq = kLargeShort;
+                    o.dzmax = kLargeShort; o.laycost = 0;
+                    store_arc<DEFO>(costs_out, a, o);
+                } else if (wt == 1 && okf[h]) {
+                    store_arc<DEFO>(costs_out, a, of[h]);
+                } else {
+                    defer(wt);
                 }
             }
         }
@@ -904,11 +925,11 @@ static int launch_costs7_v(const float *ph, const float *corr, const short *weig
     std::memset(&tm_cor, 0, sizeof(tm_cor));
     const int tma = (c7_map(tm_ph, ph, nrow, ncol, kC7WinW, kC7WinH) &&
                      c7_map(tm_cor, corr, nrow, ncol, kC7CorW, kC7CorH)) ? 1 : 0;
-    CUPHU_TRY_CUDA(cudaFuncSetAttribute(k_costs7<DEFO, FAM, MINB>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-    k_costs7<DEFO, FAM, MINB><<<nby * nbx, 256, shm, s>>>(ph, corr, weights, nrow, ncol, k, costs,
-                                                          nbx, gq, gqn, gqcap, tma, tm_ph,
-                                                          tm_cor);
+    auto kern = tma ? k_costs7<DEFO, FAM, MINB, true> : k_costs7<DEFO, FAM, MINB, false>;
+    CUPHU_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)shm));
+    kern<<<nby * nbx, 256, shm, s>>>(ph, corr, weights, nrow, ncol, k, costs, nbx, gq, gqn, gqcap,
+                                     tm_ph, tm_cor);
     return cuda_fail(cudaGetLastError(), "k_costs7");
 }
 
