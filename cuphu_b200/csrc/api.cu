@@ -465,6 +465,7 @@ static int run_job(std::vector<SceneIn> &S, const CuPhuParams &prm, const JobOpt
         P.wr = b.take<float>(np);
         P.x = b.take<double>(np);
         P.dx = jo.fp64 ? nullptr : b.take<float>(np);
+        P.bvec = jo.fp64 ? nullptr : b.take<double>(np);
         P.r = b.take<char>(np * vs);
         P.p0 = b.take<char>(np * vs);
         P.p1 = b.take<char>(np * vs);

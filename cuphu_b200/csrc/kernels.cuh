@@ -37,6 +37,9 @@ struct SolverPlanes {
     float *w0d, *w0r;           /* data weights 1/sigsq                  */
     float *wd, *wr;             /* current IRLS weights                  */
     double *x;                  /* solution, FP64 in both precisions     */
+    double *bvec;               /* mixed: right-hand side of the current IRLS
+                                   pass, stored by its assembly for the
+                                   true-residual replacements (else NULL) */
     float *dx;                  /* mixed: FP32 increment since the last fold */
     void *r, *p0, *p1;          /* PCG vectors, float or double; p is    */
     void *q, *diag;             /* double-buffered across iterations     */

@@ -366,7 +366,12 @@ __device__ __forceinline__ void dot4_df2(const float a0[4], const float b0[4], c
  * goes to zout.  Mixed mode: the FP32 residual r goes to zout (its
  * double-buffered residual plane), the preconditioner is M^-1 =
  * rcp_pre(diag32) recomputed from the weights, and the partial r.z comes
- * from dot4_df. */
+ * from dot4_df.  With P.bvec (mixed mode) the assemble pass stores the
+ * right-hand side b and the replacements of the same IRLS pass read it back
+ * instead of rebuilding it from the wrapped phase (the same doubles either
+ * way).  The thread's row and the rows above and below of x and of the arc
+ * weights arrive as 16-byte vectors; only the phase (scene layout) is read
+ * element by element.  The arithmetic and its order are the oracle's. */
 template <typename V, bool WLS>
 __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, bool zero_x,
                              bool write_diag, V *zout)
@@ -384,12 +389,34 @@ __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, b
     const float *rhsp = (WLS && P.rhs) ? P.rhs + T.pix : nullptr;
     const double eps = (double)kLapEpsF;
     const int r = q.r, nr = T.nr, nc = T.nc, pitch = T.pitch, pp = T.ph_pitch;
-    size_t prow = (size_t)r * pitch;
-    double xv[4];
+    const size_t prow = (size_t)r * pitch;
+    const bool has_dn = r < nr - 1, has_up = r > 0;
+    const bool has_l = q.c0 > 0, has_r = q.c0 + kItemVx < nc;
+    /* the down arcs of this row and of the row above (the up arcs), the
+     * right arcs of this row and the one left of the thread's columns; the
+     * last row of wd and the last column of wr are zero, so the vectors
+     * stay inside the tile's rows */
+    float wdn[4], wup[4] = {0.f, 0.f, 0.f, 0.f}, wrt[4];
+    ld4(wd + prow + q.c0, wdn);
+    if (has_up) ld4(wd + prow - pitch + q.c0, wup);
+    ld4(wr + prow + q.c0, wrt);
+    const float wlf = has_l ? ldc(wr + prow + q.c0 - 1) : 0.0f;
+    double xv[4], xdn[4] = {0.0, 0.0, 0.0, 0.0}, xup[4] = {0.0, 0.0, 0.0, 0.0};
+    double xl = 0.0, xr = 0.0;
+    if (!zero_x) {
+        ld4(x + prow + q.c0, xv);
+        if (has_dn) ld4(x + prow + pitch + q.c0, xdn);
+        if (has_up) ld4(x + prow - pitch + q.c0, xup);
+        if (has_l) xl = ldc(x + prow + q.c0 - 1);
+        if (has_r) xr = ldc(x + prow + q.c0 + kItemVx);
+    }
     V rv[4], dv[4], zv[4];
     float zf[4];   /* mixed: z = M^-1 r of the thread's pixels */
-    if (!zero_x) ld4(x + prow + q.c0, xv);
     if (!write_diag && sizeof(V) == 8) ld4(dg + prow + q.c0, dv);
+    double *bvp = P.bvec ? P.bvec + T.pix + prow + q.c0 : nullptr;
+    const bool b_stored = bvp && !write_diag;
+    double bst[4];
+    if (b_stored) ld4((const double *)bvp, bst);
     double acc = 0.0;
 #pragma unroll
     for (int j = 0; j < kItemVx; ++j) {
@@ -400,61 +427,63 @@ __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, b
             zf[j] = 0.0f;
             if (write_diag) dv[j] = (V)0;
             if (zero_x) xv[j] = 0.0;
+            bst[j] = 0.0;
             continue;
         }
-        size_t gi = (size_t)r * pp + c, pi = prow + c;
-        float pa = gdp ? 0.0f : __ldg(ph + gi);
+        const float w_dn = wdn[j], w_up = wup[j], w_rt = wrt[j];
+        const float w_lf = j == 0 ? wlf : wrt[j - 1];
         double bv = 0.0, ws = 0.0;
         float ws32 = 0.0f;   /* mixed: diag32's sum, in its order */
-        if (r < nr - 1) {
-            float w = ldc(wd + pi);
-            if (w > 0.0f) {
+        if (b_stored) {
+            bv = bst[j];
+            if (has_dn && w_dn > 0.0f) ws32 = __fadd_rn(ws32, w_dn);
+            if (has_up && w_up > 0.0f) ws32 = __fadd_rn(ws32, w_up);
+            if (c < nc - 1 && w_rt > 0.0f) ws32 = __fadd_rn(ws32, w_rt);
+            if (c > 0 && w_lf > 0.0f) ws32 = __fadd_rn(ws32, w_lf);
+        } else {
+            const size_t gi = (size_t)r * pp + c, pi = prow + c;
+            float pa = gdp ? 0.0f : __ldg(ph + gi);
+            if (has_dn && w_dn > 0.0f) {
                 float g = gdp ? ldc(gdp + pi) : lap_wrap_pi(__ldg(ph + gi + pp) - pa);
-                bv = __fma_rn(-(double)w, (double)g, bv);
-                ws += w;
-                ws32 = __fadd_rn(ws32, w);
+                bv = __fma_rn(-(double)w_dn, (double)g, bv);
+                ws += w_dn;
+                ws32 = __fadd_rn(ws32, w_dn);
             }
-        }
-        if (r > 0) {
-            float w = ldc(wd + pi - pitch);
-            if (w > 0.0f) {
+            if (has_up && w_up > 0.0f) {
                 float g = gdp ? ldc(gdp + pi - pitch) : lap_wrap_pi(pa - __ldg(ph + gi - pp));
-                bv = __fma_rn((double)w, (double)g, bv);
-                ws += w;
-                ws32 = __fadd_rn(ws32, w);
+                bv = __fma_rn((double)w_up, (double)g, bv);
+                ws += w_up;
+                ws32 = __fadd_rn(ws32, w_up);
             }
-        }
-        if (c < nc - 1) {
-            float w = ldc(wr + pi);
-            if (w > 0.0f) {
+            if (c < nc - 1 && w_rt > 0.0f) {
                 float g = grp ? ldc(grp + pi) : lap_wrap_pi(__ldg(ph + gi + 1) - pa);
-                bv = __fma_rn(-(double)w, (double)g, bv);
-                ws += w;
-                ws32 = __fadd_rn(ws32, w);
+                bv = __fma_rn(-(double)w_rt, (double)g, bv);
+                ws += w_rt;
+                ws32 = __fadd_rn(ws32, w_rt);
             }
-        }
-        if (c > 0) {
-            float w = ldc(wr + pi - 1);
-            if (w > 0.0f) {
+            if (c > 0 && w_lf > 0.0f) {
                 float g = grp ? ldc(grp + pi - 1) : lap_wrap_pi(pa - __ldg(ph + gi - 1));
-                bv = __fma_rn((double)w, (double)g, bv);
-                ws += w;
-                ws32 = __fadd_rn(ws32, w);
+                bv = __fma_rn((double)w_lf, (double)g, bv);
+                ws += w_lf;
+                ws32 = __fadd_rn(ws32, w_lf);
             }
+            if (rhsp) bv = (double)ldc(rhsp + pi);
+            bst[j] = bv;
         }
-        if (rhsp) bv = (double)ldc(rhsp + pi);
         double d = write_diag ? ws + eps : (double)dv[j];
         double y;
         if (zero_x) {
             y = 0.0;
             xv[j] = 0.0;
         } else {
-            double xa = xv[j];
+            const double xa = xv[j];
+            const double x_l = j == 0 ? xl : xv[j - 1];
+            const double x_r = j == kItemVx - 1 ? xr : xv[j + 1];
             y = eps * xa;
-            if (r < nr - 1) y = __fma_rn((double)ldc(wd + pi), xa - ldc(x + pi + pitch), y);
-            if (r > 0)      y = __fma_rn((double)ldc(wd + pi - pitch), xa - ldc(x + pi - pitch), y);
-            if (c < nc - 1) y = __fma_rn((double)ldc(wr + pi), xa - ldc(x + pi + 1), y);
-            if (c > 0)      y = __fma_rn((double)ldc(wr + pi - 1), xa - ldc(x + pi - 1), y);
+            if (has_dn)     y = __fma_rn((double)w_dn, xa - xdn[j], y);
+            if (has_up)     y = __fma_rn((double)w_up, xa - xup[j], y);
+            if (c < nc - 1) y = __fma_rn((double)w_rt, xa - x_r, y);
+            if (c > 0)      y = __fma_rn((double)w_lf, xa - x_l, y);
         }
         V rs = (V)(bv - y);
         if constexpr (sizeof(V) == 8) {
@@ -476,6 +505,7 @@ __device__ double phase_init(const TileDesc &T, int li, const SolverPlanes &P, b
     if (sizeof(V) == 8) st4(rr + prow + q.c0, rv);
     st4(zout + T.pix + prow + q.c0, zv);
     if (write_diag) st4(dg + prow + q.c0, dv);
+    if (bvp && write_diag) st4(bvp, bst);
     if (zero_x) {
         st4(x + prow + q.c0, xv);
         if (P.dx) {
