@@ -105,10 +105,34 @@ __device__ __forceinline__ double tile_reduce(const TileDesc &T, const double *p
     return tot;
 }
 
-__device__ __forceinline__ void store_partial(double acc, double *part, int item, double *sw)
+/* Partials of items [a, b) of tile T, eight items per pair of block
+ * barriers: each warp reduces its thread values of an item by block_sum's
+ * first tree and parks the warp sum; after the barrier warp k forms item
+ * k's partial by block_sum's second tree.  The partials are block_sum's of
+ * each item (the canonical tree the FP64 oracle reproduces), but warps run
+ * ahead through the eight items instead of meeting at two barriers per
+ * item.  f(li) returns the thread's value of item li. */
+constexpr int kItemGroup = 8;
+template <typename F>
+__device__ __forceinline__ void item_partials(const TileDesc &T, int a, int b, double *part,
+                                              double (*sgrp)[8], F &&f)
 {
-    double bs = block_sum(acc, sw);
-    if (threadIdx.x == 0) part[item] = bs;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int g0 = a; g0 < b; g0 += kItemGroup) {
+        const int n = min(kItemGroup, b - g0);
+        for (int k = 0; k < n; ++k) {
+            double v = f(g0 + k);
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+            if (lane == 0) sgrp[k][w] = v;
+        }
+        __syncthreads();
+        if (w < n) {
+            double v = lane < (int)(blockDim.x >> 5) ? sgrp[w][lane] : 0.0;
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+            if (lane == 0) part[T.item0 + g0 + w] = v;
+        }
+        __syncthreads();
+    }
 }
 
 /* block tree without the leading barrier, for item loops: consecutive items
@@ -1557,6 +1581,7 @@ __global__ void __launch_bounds__(kItemThreads, MINB)
     extern __shared__ __align__(128) char dsm_raw[];
     __shared__ double sw[32];
     __shared__ double red[2][kNComp][8];   /* mixed: warp partials by item parity */
+    __shared__ double sgrp[kItemGroup][8];   /* warp sums of a group of items */
     __shared__ double s_bcast;
     __shared__ int s_flag;
     __shared__ __align__(8) uint64_t bars[NS];
@@ -1592,10 +1617,9 @@ __global__ void __launch_bounds__(kItemThreads, MINB)
             const TileDesc &T = stile(sc, tiles, t);
             int a, b;
             slice_items(sc, T, t, a, b);
-            for (int li = a; li < b; ++li)
-                store_partial(phase_init<V, WLS>(T, li, P, outer == 0 && !(WLS && sp.warm), true,
-                                                 zb[0]),
-                              pbuf[pc & 1], T.item0 + li, sw);
+            const bool zx = outer == 0 && !(WLS && sp.warm);
+            item_partials(T, a, b, pbuf[pc & 1], sgrp,
+                          [&](int li) { return phase_init<V, WLS>(T, li, P, zx, true, zb[0]); });
             if (b > a) seg_done(T, t, b - a, pbuf[pc & 1], tbuf[pc & 1], tick, sw, &s_bcast, &s_flag);
         }
         ++pc;
@@ -1744,9 +1768,9 @@ __global__ void __launch_bounds__(kItemThreads, MINB)
                         if (sc.pre[t + 1] == sc.pre[t]) continue;
                         int a, b;
                         slice_items(sc, T, t, a, b);
-                        for (int li = a; li < b; ++li)
-                            store_partial(phase_init<V, WLS>(T, li, P, false, false, zb[zsel]),
-                                          pbuf[pc & 1], T.item0 + li, sw);
+                        item_partials(T, a, b, pbuf[pc & 1], sgrp, [&](int li) {
+                            return phase_init<V, WLS>(T, li, P, false, false, zb[zsel]);
+                        });
                         if (b > a)
                             seg_done(T, t, b - a, pbuf[pc & 1], tbuf[pc & 1], tick, sw, &s_bcast,
                                      &s_flag);
