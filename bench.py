@@ -42,10 +42,15 @@ METRIC = "Mpix/s unwrapped at 8192^2 (mixed-precision Laplace PCG)"
 
 
 # measured k_solve DRAM bytes (mixed precision), see the roofline block:
-# ncu dram__bytes_read.sum + dram__bytes_write.sum of the 4096^2 case at 20
-# and 40 PCG iterations (one pass): 17.69 and 33.65 GB
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of the 4096^2 case (4 x 4
+# tiles, 18.39 M tile pixels) at 20, 40 and 60 PCG iterations of one pass:
+# 17.84, 33.80 and 50.52 GB.  40 - 20: the marginal bytes per pixel-iteration;
+# 20 iterations' intercept: the fixed bytes per tile pixel of a pass
+# (assembly, fold, final); 60 - 40 beyond 20 iterations: the one true-residual
+# replacement (at iteration 50)
 TRAFFIC_PER_PX_ITER = 43.4
-TRAFFIC_PER_PASS_PX = 94.3
+TRAFFIC_PER_PASS_PX = 102.3
+TRAFFIC_PER_REPL_PX = 40.8
 
 
 def hbm_peak():
@@ -679,7 +684,8 @@ def run_ours(args, rank, world, local_rank):
 
     # roofline of the dominant kernel (the persistent solve): algorithmic
     # bytes = tile pixels x (36 B per PCG iteration x iterations of the
-    # active tiles + 38 B per IRLS pass for assemble and reweight)
+    # active tiles + 38 B per IRLS pass for assemble and reweight + 12 B per
+    # true-residual replacement, one SpMV read of x and the weights)
     peak, peak_kind = hbm_peak()
     # tile extents of the reference's tile geometry (cuphu_solver.cpp:1753-1791)
     tr_f = [(int(t * (nrow - 64) / ntr), (nrow if t == ntr - 1 else int((t + 1) * (nrow - 64) / ntr) + 64)) for t in range(ntr)]
@@ -687,14 +693,18 @@ def run_ours(args, rank, world, local_rank):
     tile_px = sum((b - a) for a, b in tr_f) * sum((b - a) for a, b in tc_f)
     px_iters = st.px_iters                # iterations x pixels of the active tiles
     bpi = 36 if prec == 0 else 64
-    alg_bytes = px_iters * bpi + (opts.n_irls + 1) * tile_px * 38
+    # pixels of the replacements: every tile replaces its residual once per
+    # replace_every of its iterations (mixed precision only)
+    repl_px = px_iters / opts.replace_every if prec == 0 and opts.replace_every > 0 else 0.0
+    alg_bytes = px_iters * bpi + (opts.n_irls + 1) * tile_px * 38 + repl_px * 12
     achieved = alg_bytes / (st.solve_ms * 1e-3) / 1e9
     # DRAM traffic per launch, scaled from ncu captures of the 4096^2 case
-    # (dram__bytes_read.sum + dram__bytes_write.sum at 20 and 40 iterations):
-    # the marginal bytes per active-tile pixel-iteration plus the fixed bytes
-    # per tile pixel of each IRLS pass (assemble/INIT and final)
+    # (dram__bytes_read.sum + dram__bytes_write.sum at 20, 40 and 60
+    # iterations): the marginal bytes per active-tile pixel-iteration, the
+    # fixed bytes per tile pixel of each IRLS pass (assemble/INIT and final)
+    # and the bytes per pixel of a true-residual replacement
     traffic = (px_iters * TRAFFIC_PER_PX_ITER + (opts.n_irls + 1) * tile_px * TRAFFIC_PER_PASS_PX
-               if prec == 0 else None)
+               + repl_px * TRAFFIC_PER_REPL_PX if prec == 0 else None)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                 "kernel": "k_solve", "solve_ms": st.solve_ms, "pcg_iterations": st.total_iters,
