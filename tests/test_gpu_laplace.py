@@ -79,6 +79,37 @@ def test_mixed_close_to_oracle_on_config_like_scene(torch_cuda):
     assert np.sum(gk != k) <= max(3, int(1e-4 * k.size))
 
 
+@pytest.mark.parametrize("replace_every", [1, 3, 7, 0])
+def test_mixed_residual_replacement_period(torch_cuda, replace_every):
+    """The true-residual replacement (fold dx into x, r = b - A x from the
+    right-hand side the IRLS pass's assembly stored) run every 1, 3 or 7
+    iterations, and never (0): the mixed solve must stay within the same bar
+    against the FP64 oracle as with the default period of 50, and runs that
+    replace every iteration take as many iterations as the default within a
+    few per cent."""
+    ph, g, _ = scene(160, 200, 13, nlooks=5.0)
+    costs = O.build_costs(ph, g, 5.0, mode=1)
+    x, k, _, iters = O.laplace_f64(costs, ph, O.lap_opts(n_irls=3))
+    nr, nc = ph.shape
+    dcost, dph = to_dev(costs), to_dev(ph)
+    du = empty((nr, nc), torch_cuda.float32)
+    dk = empty((nr, nc), torch_cuda.int32)
+    dcont = empty((nr, nc), torch_cuda.float32)
+    o = default_solve_options(precision=0, n_irls=3)
+    o.replace_every = replace_every
+    st = CuPhuSolveStats()
+    check(lib().cuphu_laplace_solve_device(dptr(dcost), costs.shape[1], dptr(dph), nr, nc,
+                                           C.byref(o), dptr(du), dptr(dk), dptr(dcont),
+                                           C.byref(st), None))
+    gk, gc = to_host(dk), to_host(dcont)
+    off = float(ph[0, 0]) - x[0, 0]
+    rms = float(np.sqrt(np.mean((gc.astype(np.float64) - (x + off)) ** 2)))
+    assert rms < 1e-3, rms
+    assert np.sum(gk != k) <= max(3, int(1e-4 * k.size))
+    assert abs(st.total_iters - int(iters.sum())) <= max(8, int(0.1 * iters.sum())), \
+        (st.total_iters, int(iters.sum()))
+
+
 def test_solver_is_deterministic(torch_cuda):
     ph, g, _ = scene(200, 240, 5)
     costs = O.build_costs(ph, g, 5.0, mode=0)
