@@ -421,7 +421,7 @@ struct C7Smem {
     float2 dpp[kC7W * kC7PP];             /* difference pairs */
     alignas(128) float cor[kC7CorH * kC7CorW];   /* coherence window (TMA path) */
     C7Deferred q[kC7Q];
-    short lay[kC7Tab];
+    alignas(8) short lay[kC7Tab];
     unsigned long long bar;
     int qn;
     unsigned gbase;
@@ -630,6 +630,7 @@ __global__ void __launch_bounds__(256, MINB) k_costs7(const float *__restrict__ 
                                                    void *__restrict__ costs_out, int nbx,
                                                    C7Global *__restrict__ gq, unsigned *gqn,
                                                    unsigned gqcap,
+                                                   const short *__restrict__ laytab,
                                                    const __grid_constant__ CUtensorMap tm_ph,
                                                    const __grid_constant__ CUtensorMap tm_cor)
 {
@@ -644,11 +645,19 @@ __global__ void __launch_bounds__(256, MINB) k_costs7(const float *__restrict__ 
     const int r0 = by * kC7B, c0 = bx * kC7B;
     const int tid = threadIdx.x;
     if (tid == 0) S.qn = 0;
-    /* laycost of every sigsq the fast path can produce */
+    /* laycost of every sigsq the fast path can produce: the launch's table
+     * (k_c7_laytab), four entries per thread, or computed here when the
+     * launch has no scratch for it */
     const int ntab = DEFO ? min(max(k.s_rho0, k.sigsqshortmin) + 1, kC7Tab) : 0;
-    if (DEFO)
-        for (int v = tid; v < ntab; v += blockDim.x)
-            S.lay[v] = (short)min(isqrt_floor(k.dzmax * v), (int)SHRT_MAX);
+    if (DEFO) {
+        if (laytab) {
+            static_assert(kC7Tab == 4 * 256, "one short4 of the table per thread");
+            reinterpret_cast<short4 *>(S.lay)[tid] = __ldg(reinterpret_cast<const short4 *>(laytab) + tid);
+        } else {
+            for (int v = tid; v < ntab; v += blockDim.x)
+                S.lay[v] = (short)min(isqrt_floor(k.dzmax * v), (int)SHRT_MAX);
+        }
+    }
 
     constexpr int NR = kC7W + (FAM == 0 ? 1 : 0);             /* phase rows */
     constexpr int NP = kC7W - kC7H + (FAM == 1 ? 1 : 0);      /* phase pairs per row */
@@ -864,6 +873,17 @@ __global__ void __launch_bounds__(256, MINB) k_costs7(const float *__restrict__ 
     }
 }
 
+/* the laycost table of a launch: entry v = (int)sqrt(dzmax v) of the
+ * reference (cuphu_cost.cu:225-265), clamped to SHRT_MAX, for every sigsq
+ * the fast path can produce (entries past that are zero and never read) */
+__global__ void __launch_bounds__(256) k_c7_laytab(short *__restrict__ tab, const CostConsts k)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= kC7Tab) return;
+    const int ntab = min(max(k.s_rho0, k.sigsqshortmin) + 1, kC7Tab);
+    tab[v] = v < ntab ? (short)min(isqrt_floor(k.dzmax * v), (int)SHRT_MAX) : (short)0;
+}
+
 template <bool DEFO>
 __global__ void __launch_bounds__(256) k_costs7_drain(const C7Global *__restrict__ gq,
                                                       const unsigned *__restrict__ gqn,
@@ -914,7 +934,7 @@ static bool c7_map(CUtensorMap &m, const float *base, int nrow, int ncol, int bx
 template <bool DEFO, int FAM, int MINB>
 static int launch_costs7_v(const float *ph, const float *corr, const short *weights, int nrow,
                            int ncol, const CostConsts &k, void *costs, C7Global *gq,
-                           unsigned *gqn, unsigned gqcap, cudaStream_t s)
+                           unsigned *gqn, unsigned gqcap, const short *laytab, cudaStream_t s)
 {
     const int dr = FAM == 0 ? nrow - 1 : nrow, dc = FAM == 0 ? ncol : ncol - 1;
     if (dr < 1 || dc < 1) return 0;
@@ -929,7 +949,7 @@ static int launch_costs7_v(const float *ph, const float *corr, const short *weig
     CUPHU_TRY_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)shm));
     kern<<<nby * nbx, 256, shm, s>>>(ph, corr, weights, nrow, ncol, k, costs, nbx, gq, gqn, gqcap,
-                                     tm_ph, tm_cor);
+                                     laytab, tm_ph, tm_cor);
     return cuda_fail(cudaGetLastError(), "k_costs7");
 }
 
@@ -937,16 +957,16 @@ static int launch_costs7_v(const float *ph, const float *corr, const short *weig
 template <bool DEFO, int FAM>
 static int launch_costs7_t(const float *ph, const float *corr, const short *weights, int nrow,
                            int ncol, const CostConsts &k, void *costs, C7Global *gq,
-                           unsigned *gqn, unsigned gqcap, cudaStream_t s)
+                           unsigned *gqn, unsigned gqcap, const short *laytab, cudaStream_t s)
 {
     int dev = 0;
     cudaGetDevice(&dev);
     const long long arcs = 2LL * nrow * ncol;
     if (tune_get(dev, 0, arcs) == 1)
         return launch_costs7_v<DEFO, FAM, 4>(ph, corr, weights, nrow, ncol, k, costs, gq, gqn,
-                                             gqcap, s);
+                                             gqcap, laytab, s);
     return launch_costs7_v<DEFO, FAM, 3>(ph, corr, weights, nrow, ncol, k, costs, gq, gqn, gqcap,
-                                         s);
+                                         laytab, s);
 }
 
 /* both arc families, then the queued arcs; the queue (about one arc in 128
@@ -959,18 +979,30 @@ static int launch_costs7_all(const float *ph, const float *corr, const short *we
     const unsigned long long narcs =
         (unsigned long long)(nrow - 1) * ncol + (unsigned long long)nrow * (ncol - 1);
     const unsigned cap = (unsigned)std::min<unsigned long long>(narcs / 128 + 4096, 1u << 24);
+    /* scratch: the queue counter, the laycost table (DEFO), the queue */
+    constexpr size_t kTabOff = 256, kQueueOff = kTabOff + kC7Tab * sizeof(short);
+    static_assert(kQueueOff % 256 == 0, "queue offset");
     void *buf = nullptr;
     C7Global *gq = nullptr;
     unsigned *gqn = nullptr;
-    if (cudaMallocAsync(&buf, (size_t)cap * sizeof(C7Global) + 256, s) == cudaSuccess) {
+    short *laytab = nullptr;
+    if (cudaMallocAsync(&buf, (size_t)cap * sizeof(C7Global) + kQueueOff, s) == cudaSuccess) {
         gqn = reinterpret_cast<unsigned *>(buf);
-        gq = reinterpret_cast<C7Global *>(static_cast<char *>(buf) + 256);
+        gq = reinterpret_cast<C7Global *>(static_cast<char *>(buf) + kQueueOff);
         CUPHU_TRY_CUDA(cudaMemsetAsync(gqn, 0, sizeof(unsigned), s));
+        if (DEFO) {
+            laytab = reinterpret_cast<short *>(static_cast<char *>(buf) + kTabOff);
+            k_c7_laytab<<<kC7Tab / 256, 256, 0, s>>>(laytab, k);
+            CUPHU_TRY_CUDA(cudaGetLastError());
+        }
     } else {
         cudaGetLastError();
     }
-    int rc = launch_costs7_t<DEFO, 0>(ph, corr, weights, nrow, ncol, k, costs, gq, gqn, cap, s);
-    if (!rc) rc = launch_costs7_t<DEFO, 1>(ph, corr, weights, nrow, ncol, k, costs, gq, gqn, cap, s);
+    int rc = launch_costs7_t<DEFO, 0>(ph, corr, weights, nrow, ncol, k, costs, gq, gqn, cap, laytab,
+                                      s);
+    if (!rc)
+        rc = launch_costs7_t<DEFO, 1>(ph, corr, weights, nrow, ncol, k, costs, gq, gqn, cap,
+                                      laytab, s);
     if (!rc && gq) {
         k_costs7_drain<DEFO><<<148 * 4, 256, 0, s>>>(gq, gqn, cap, k, costs);
         rc = cuda_fail(cudaGetLastError(), "k_costs7_drain");
